@@ -1,0 +1,159 @@
+/*
+ * shtensor_b200.h -- C ABI of the B200 (sm_100a) block-sparse tensor contraction library.
+ *
+ * Drop-in boundary for shtensor's single-rank contraction path.  Every entry point returns
+ * an sht_status (0 = success) and never throws; the message of the last failure on the
+ * calling thread is returned by sht_last_error().  Handles are opaque.  Device memory for
+ * tensors, plans and scratch comes from the context's device pool.  A context and the
+ * handles made from it are not thread-safe: one host thread drives a context at a time.
+ * Stream arguments are cudaStream_t values passed as void* (NULL = the legacy default stream).
+ *
+ * Reference interfaces each entry point replaces (paths relative to the shtensor root):
+ *   sht_init / sht_finalize      Context(MPI_Comm, int64_t pool_bytes)   src/Shmem/Context.h:30
+ *   sht_pool_*                   MemoryPool::{allocate,reallocate,free,get_free_mem}
+ *                                src/Shmem/MemoryPool.h:51-96,126-354
+ *   sht_kernel_create            Kernel<T>::Kernel(expr, sizes_in1, sizes_in2, sizes_out,
+ *                                alpha, beta, KernelType)               src/Kernel/Kernel.h:69-86
+ *   sht_kernel_call              Kernel<T>::call(T* a, T* b, T* c, int64_t nb_ops)
+ *                                                                       src/Kernel/Kernel.h:88-91
+ *   sht_kernel_info              KernelBase::get_info()                 src/Kernel/Kernel.cpp:29-32
+ *   sht_tensor_create            Tensor<T,N>(ctx, VArray<N> block_sizes) src/Tensor/Tensor.h:27-32
+ *   sht_tensor_reserve(_all)     BaseTensor::reserve / reserve_all      src/Tensor/BaseTensor.cpp:97-251
+ *   sht_tensor_get_index         BaseTensor::get_sparse_info()          src/Tensor/BaseTensor.h:51
+ *   sht_tensor_upload/download   block data access (get_local_block, iterators)
+ *                                                                       src/Tensor/Tensor.h:38-52,75-258
+ *   sht_tensor_norms             BlockSpan::get_norm                    src/Basics/BlockSpan.h:140-164
+ *   sht_tensor_filter            Tensor<T,N>::filter(eps, norm, compress) src/Tensor/Tensor.h:337-363
+ *   sht_tensor_compress          BaseTensor::compress                   src/Tensor/BaseTensor.cpp:253-354
+ *   sht_contract, sht_plan_*     the block-sparse contract the reference lacks
+ *                                (src/Tensor/Tensor.cpp is empty; test/test_contract.cpp:5-23)
+ *   sht_server_*                 serving loop (no reference counterpart)
+ */
+#ifndef SHTENSOR_B200_H
+#define SHTENSOR_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+  SHT_OK = 0,
+  SHT_ERR_INVALID = 1,      /* bad argument or handle */
+  SHT_ERR_PARSE = 2,        /* einsum expression rejected */
+  SHT_ERR_SIZE = 3,         /* size / block-size mismatch */
+  SHT_ERR_OOM = 4,          /* device pool exhausted */
+  SHT_ERR_CUDA = 5,         /* CUDA runtime error */
+  SHT_ERR_TIMEOUT = 6,      /* a bounded device or host wait expired */
+  SHT_ERR_UNSUPPORTED = 7,  /* valid request outside the implemented envelope */
+  SHT_ERR_STATE = 8         /* operation not valid in the handle's current state */
+} sht_status;
+
+typedef enum { SHT_F32 = 0, SHT_F64 = 1 } sht_dtype;                 /* FloatType, Definitions.h:44-48 */
+typedef enum { SHT_KERNEL_LAPACK = 0, SHT_KERNEL_XMM = 1 } sht_kernel_type; /* KernelType, KernelDefinitions.h:11-15 */
+typedef enum {
+  SHT_NORM_FROBENIUS = 0,            /* sqrt(sum v^2), fixed 32-way strided order */
+  SHT_NORM_MAXABS = 1,
+  SHT_NORM_FROBENIUS_REFCOMPAT = 2   /* the reference's int-accumulator evaluation */
+} sht_norm;
+typedef enum {
+  SHT_MODE_PLAIN_FP64 = 0,   /* output-stationary FP64 DFMA tiles, one launch, bit-exact order */
+  SHT_MODE_BATCHED_FP64 = 1, /* persistent kernel over a size-class work list, tuned tiles */
+  SHT_MODE_SPLIT = 2         /* split-precision (Ozaki) INT8 tensor-core slices, FP64 reassembly */
+} sht_mode;
+
+typedef struct sht_ctx sht_ctx;
+typedef struct sht_kernel sht_kernel;
+typedef struct sht_tensor sht_tensor;
+typedef struct sht_plan sht_plan;
+
+typedef struct {
+  int64_t npairs;       /* surviving block pairs */
+  int64_t nblocks_c;    /* C blocks after the contraction */
+  int64_t nnz_c;        /* C elements after the contraction */
+  int64_t nwork;        /* tiles launched */
+  double flops;         /* sum over pairs of 2*m*n*k */
+  double plan_ms;       /* host-timed plan phase (matching, pattern, work list) */
+  double exec_ms;       /* device-timed execute phase (0 unless timing was requested) */
+  int32_t slices;       /* split mode: INT8 slices per operand (0 otherwise) */
+  int32_t reserved;
+} sht_contract_report;
+
+/* ---- context and device pool (Context / MemoryPool) ---- */
+sht_status sht_init(sht_ctx** ctx, int device, size_t pool_bytes);
+sht_status sht_finalize(sht_ctx* ctx);
+const char* sht_last_error(void);
+sht_status sht_pool_info(sht_ctx* ctx, size_t* capacity, size_t* free_bytes, size_t* chunk_header,
+                         size_t* alignment);
+sht_status sht_pool_alloc(sht_ctx* ctx, size_t bytes, void** dptr);
+sht_status sht_pool_realloc(sht_ctx* ctx, void** dptr, size_t bytes, void* stream);
+sht_status sht_pool_free(sht_ctx* ctx, void* dptr, void* stream);
+/* accounting parameters (chunk header bytes, alignment); only on an empty pool */
+sht_status sht_pool_configure(sht_ctx* ctx, size_t chunk_header, size_t alignment);
+
+/* ---- per-block stack kernel (Kernel<T>) ---- */
+sht_status sht_kernel_create(sht_ctx* ctx, const char* expr, const int* sizes_a, int na,
+                             const int* sizes_b, int nb, const int* sizes_c, int nc, double alpha,
+                             double beta, sht_dtype dtype, sht_kernel_type type, sht_kernel** out);
+/* a, b, c: nb_ops contiguous same-shape blocks each, column-major.  Device pointers run in
+ * place on `stream`; host pointers are staged through the pool and the call returns after
+ * the result is back in host memory. */
+sht_status sht_kernel_call(sht_kernel* k, const void* a, const void* b, void* c, int64_t nb_ops,
+                           void* stream);
+sht_status sht_kernel_info(sht_kernel* k, char* buf, size_t len);
+sht_status sht_kernel_destroy(sht_kernel* k);
+
+/* ---- block-sparse tensors (Tensor<T,N>) ---- */
+/* nblk[d] blocks in mode d; block_sizes holds the sizes of mode 0, then mode 1, ... */
+sht_status sht_tensor_create(sht_ctx* ctx, int order, const int* nblk, const int* block_sizes,
+                             sht_dtype dtype, sht_tensor** out);
+/* idx is mode-major like VArray<N>: idx[d*nblocks + b]; zero-fills the data */
+sht_status sht_tensor_reserve(sht_tensor* t, int64_t nblocks, const int* idx);
+sht_status sht_tensor_reserve_all(sht_tensor* t);
+sht_status sht_tensor_info(const sht_tensor* t, int64_t* nblocks, int64_t* nnz);
+/* host copies of the sparse index: sorted rolled ids, element offsets, rows (nblk[0]) */
+sht_status sht_tensor_get_index(sht_tensor* t, int64_t* ids, int64_t* offsets, int64_t* rows);
+sht_status sht_tensor_upload(sht_tensor* t, const void* host, int64_t nelem, void* stream);
+sht_status sht_tensor_download(sht_tensor* t, void* host, int64_t nelem, void* stream);
+sht_status sht_tensor_device_data(sht_tensor* t, void** dptr);
+sht_status sht_tensor_norms(sht_tensor* t, sht_norm norm, double* host_out, void* stream);
+sht_status sht_tensor_filter(sht_tensor* t, double eps, sht_norm norm, int compress, void* stream);
+sht_status sht_tensor_compress(sht_tensor* t, void* stream);
+sht_status sht_tensor_destroy(sht_tensor* t);
+
+/* ---- block-sparse contraction: C = beta*C + alpha * contract(expr, A, B) ---- */
+/* pairs with norm(a)*norm(b) < screen_eps are dropped (screen_eps <= 0 keeps all) */
+sht_status sht_contract(sht_ctx* ctx, const char* expr, double alpha, sht_tensor* A,
+                        sht_tensor* B, double beta, sht_tensor* C, double screen_eps,
+                        sht_norm norm, sht_mode mode, void* stream, sht_contract_report* rep);
+/* plan = matching + C pattern (C is re-reserved to the result pattern) + work list */
+sht_status sht_plan_create(sht_ctx* ctx, const char* expr, sht_tensor* A, sht_tensor* B,
+                           sht_tensor* C, double screen_eps, sht_norm norm, sht_mode mode,
+                           void* stream, sht_plan** out);
+sht_status sht_plan_execute(sht_plan* p, double alpha, double beta, void* stream);
+/* captures sht_plan_execute into a CUDA graph on first use and replays it after */
+sht_status sht_plan_execute_graph(sht_plan* p, double alpha, double beta, void* stream);
+sht_status sht_plan_report(sht_plan* p, sht_contract_report* rep);
+/* pair list as (idC, idA, idB) triples by block id, in execution order */
+sht_status sht_plan_pairs(sht_plan* p, int64_t* triples, int64_t capacity);
+sht_status sht_plan_destroy(sht_plan* p);
+
+/* ---- split-precision error report (max abs and relative Frobenius vs an FP64 result) ---- */
+sht_status sht_tensor_compare(sht_tensor* X, sht_tensor* Ref, double* max_abs, double* rel_fro,
+                              void* stream);
+
+/* ---- autotuner ---- */
+/* sweeps tile shapes per (m,n,k) size class of the plan and stores the choice; file may be NULL */
+sht_status sht_autotune(sht_plan* p, const char* cache_file, void* stream);
+
+/* ---- diagnostics ---- */
+/* which = 0: FP64 FMA peak of this GPU in TFLOP/s (the FP64 kernels' roofline denominator) */
+sht_status sht_measure_peak(sht_ctx* ctx, int which, double* value);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

@@ -1,0 +1,53 @@
+// contract.h -- plan object and entry points of the block-sparse contraction.
+#pragma once
+
+#include "sht_internal.h"
+#include "tile_types.h"
+
+struct sht_plan {
+  sht_ctx* ctx = nullptr;
+  sht_mode mode = SHT_MODE_PLAIN_FP64;
+  sht_tensor *A = nullptr, *B = nullptr, *C = nullptr;
+  ShtMaps maps;
+  sht::TileMaps tmaps{};
+  long long npairs = 0, ncblk = 0, nwork = 0, nwork_touched = 0;
+  double flops = 0.0, plan_ms = 0.0, exec_ms = 0.0;
+  int shape = 0, work_tm = 64, work_tn = 64;
+  sht::PoolBuf d_pair_a, d_pair_b;  // int32 storage indices into A / B, canonical order
+  sht::PoolBuf d_pstart;            // int32[ncblk + 1]
+  sht::PoolBuf d_work;              // int2 (C block, tile) for the plain path
+  // batched path
+  sht::PoolBuf d_bwork;             // int4 (C block, tile, class, 0)
+  sht::PoolBuf d_counter;           // work counter of the persistent kernel
+  long long bwork = 0, bwork_touched = 0;
+  int bclass_shape[8] = {0};
+  int nclass = 0;
+  // split path
+  sht::PoolBuf d_split;             // slices and scales (split mode)
+  int split_slices = 0;
+  // graph replay
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t graph_exec = nullptr;
+  double graph_alpha = 0.0, graph_beta = 0.0;
+  ~sht_plan() {
+    if (graph_exec) cudaGraphExecDestroy(graph_exec);
+    if (graph) cudaGraphDestroy(graph);
+  }
+};
+
+namespace sht {
+
+struct SparseArgs;
+
+sht_plan* plan_create(sht_ctx* ctx, const std::string& expr, sht_tensor* A, sht_tensor* B, sht_tensor* C,
+                      double eps, sht_norm norm, sht_mode mode, cudaStream_t s);
+void build_work(sht_plan* p, int TM, int TN, cudaStream_t s);
+void plan_execute(sht_plan* p, double alpha, double beta, cudaStream_t s);
+void batched_prepare(sht_plan* p, cudaStream_t s);
+void batched_execute(sht_plan* p, const SparseArgs& g, long long nwork_plain, cudaStream_t s);
+void block_dims_sizes(const sht_tensor* t, const long long* ids, long long n, int* dims, long long* sizes,
+                      cudaStream_t s);
+void tensor_compress_device(sht_tensor* t, cudaStream_t s);
+void tensor_filter_device(sht_tensor* t, double eps, sht_norm norm, int compress, cudaStream_t s);
+
+}  // namespace sht

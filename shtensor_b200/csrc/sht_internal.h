@@ -1,0 +1,181 @@
+// sht_internal.h -- internal types shared by the host runtime and the CUDA kernels.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <cstdio>
+#include <map>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "../../include/shtensor_b200.h"
+
+namespace sht {
+
+constexpr int kMaxOrder = 8;
+
+// ---------------------------------------------------------------------------------------
+// errors: every C entry point converts a thrown Error into its status + thread-local text
+// ---------------------------------------------------------------------------------------
+struct Error {
+  sht_status code;
+  std::string msg;
+};
+[[noreturn]] void fail(sht_status code, const std::string& msg);
+void set_last_error(const std::string& msg);
+
+#define SHT_CUDA(call)                                                                    \
+  do {                                                                                    \
+    cudaError_t e_ = (call);                                                              \
+    if (e_ != cudaSuccess)                                                                \
+      ::sht::fail(SHT_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_));      \
+  } while (0)
+
+inline cudaStream_t as_stream(void* s) { return reinterpret_cast<cudaStream_t>(s); }
+
+// ---------------------------------------------------------------------------------------
+// Device pool.  One cudaMalloc arena, first-fit chunk list kept on the host, with the
+// accounting of the reference's MemoryPool (src/Shmem/MemoryPool.h:126-354): each chunk
+// costs `header` bytes, data sizes are rounded up to `align`, frees coalesce both sides.
+// Frees are stream-ordered: a freed chunk carries the event recorded on the freeing stream
+// and the next allocation from it makes its own stream wait on that event.
+// ---------------------------------------------------------------------------------------
+class DevicePool {
+ public:
+  DevicePool(int device, size_t bytes);
+  ~DevicePool();
+  void* allocate(size_t bytes, cudaStream_t stream);
+  void free(void* p, cudaStream_t stream);
+  void* reallocate(void* p, size_t bytes, cudaStream_t stream);
+  size_t size_of(void* p) const;
+  size_t capacity() const { return cap_; }
+  size_t free_bytes() const { return free_; }
+  size_t header() const { return header_; }
+  size_t alignment() const { return align_; }
+  void configure(size_t header, size_t align);
+  bool owns(const void* p) const;
+
+ private:
+  struct Chunk {
+    size_t size = 0;  // data bytes (header excluded)
+    bool free = true;
+    std::vector<cudaEvent_t> pending;
+  };
+  // chunk start offset (its header starts here; data at off + header) -> chunk
+  std::map<size_t, Chunk> chunks_;
+  char* base_ = nullptr;
+  size_t cap_ = 0, free_ = 0, header_ = 256, align_ = 256;
+  std::vector<cudaEvent_t> spare_events_;
+  cudaEvent_t take_event();
+  void wait_pending(Chunk& c, cudaStream_t stream);
+  std::map<size_t, Chunk>::iterator find_data(const void* p);
+};
+
+// RAII pool buffer
+struct PoolBuf {
+  DevicePool* pool = nullptr;
+  void* ptr = nullptr;
+  size_t bytes = 0;
+  cudaStream_t stream = nullptr;
+  PoolBuf() = default;
+  PoolBuf(DevicePool* p, size_t b, cudaStream_t s) : pool(p), bytes(b), stream(s) {
+    ptr = b ? p->allocate(b, s) : nullptr;
+  }
+  PoolBuf(const PoolBuf&) = delete;
+  PoolBuf& operator=(const PoolBuf&) = delete;
+  PoolBuf(PoolBuf&& o) noexcept { *this = std::move(o); }
+  PoolBuf& operator=(PoolBuf&& o) noexcept {
+    if (this != &o) {
+      release();
+      pool = o.pool; ptr = o.ptr; bytes = o.bytes; stream = o.stream;
+      o.ptr = nullptr; o.bytes = 0;
+    }
+    return *this;
+  }
+  ~PoolBuf() { release(); }
+  void release() {
+    if (ptr && pool) pool->free(ptr, stream);
+    ptr = nullptr;
+    bytes = 0;
+  }
+  template <typename T> T* as() const { return static_cast<T*>(ptr); }
+  // the stream whose work must finish before the memory is reused
+  void use_on(cudaStream_t s) { stream = s; }
+};
+
+}  // namespace sht
+
+// ---------------------------------------------------------------------------------------
+// handles
+// ---------------------------------------------------------------------------------------
+struct sht_ctx {
+  int device = 0;
+  int num_sms = 148;
+  std::unique_ptr<sht::DevicePool> pool;
+  cudaStream_t stage_stream = nullptr;  // host-staging copies
+  std::map<std::string, int> tuned;     // autotuner choices: size-class key -> tile id
+};
+
+// Parsed einsum: matrix dimension <-> tensor modes (local positions)
+struct ShtMaps {
+  std::vector<int> rowA, colA, rowB, colB, rowC, colC;
+};
+
+struct sht_kernel {
+  sht_ctx* ctx = nullptr;
+  std::string expr;
+  std::vector<int> sa, sb, sc;
+  ShtMaps maps;
+  double alpha = 1.0, beta = 0.0;
+  sht_dtype dtype = SHT_F64;
+  sht_kernel_type type = SHT_KERNEL_XMM;
+  int64_t m = 0, n = 0, k = 0, size_a = 0, size_b = 0, size_c = 0;
+};
+
+struct sht_tensor {
+  sht_ctx* ctx = nullptr;
+  int order = 0;
+  sht_dtype dtype = SHT_F64;
+  std::vector<std::vector<int>> bs;
+  std::vector<int> nblk;
+  std::vector<int64_t> gstride;
+  // host index (authoritative unless host_stale)
+  std::vector<int64_t> ids, offsets, rows;
+  bool host_stale = false;
+  int64_t nblocks = 0, nnz = 0;
+  // device arrays
+  sht::PoolBuf d_bsizes;   // int32, concatenated per mode
+  sht::PoolBuf d_bstart;   // int32[order], start of each mode in d_bsizes
+  sht::PoolBuf d_ids;      // int64[nblocks]
+  sht::PoolBuf d_offsets;  // int64[nblocks]
+  sht::PoolBuf d_dims;     // int32[nblocks*order]
+  sht::PoolBuf d_data;     // elements
+  size_t esize() const { return dtype == SHT_F64 ? 8 : 4; }
+};
+
+namespace sht {
+
+// einsum parsing (einsum.cpp)
+void parse_einsum(const std::string& expr, int nA, const int* sA, int nB, const int* sB, int nC,
+                  const int* sC, ShtMaps& m);
+
+// tensors (tensor.cu)
+void tensor_set_index(sht_tensor* t, std::vector<int64_t>&& ids, cudaStream_t s);
+void tensor_sync_host(sht_tensor* t, cudaStream_t s);
+void tensor_upload_index(sht_tensor* t, cudaStream_t s);
+void tensor_norms_device(sht_tensor* t, sht_norm norm, double* d_out, cudaStream_t s);
+// Record that `s` uses the tensor's device buffers: when they are freed, reuse of the memory
+// is ordered after the work queued on `s` so far.
+void tensor_touch(sht_tensor* t, cudaStream_t s);
+int64_t block_size_of(const sht_tensor* t, int64_t id);
+
+// stack kernel (stack.cu)
+void stack_call(sht_kernel* k, const void* a, const void* b, void* c, int64_t nb_ops,
+                cudaStream_t s);
+
+// timing helpers
+double now_ms();
+
+}  // namespace sht
