@@ -109,7 +109,7 @@ void tensor_sync_host(sht_tensor* t, cudaStream_t s) {
   SHT_CUDA(cudaStreamSynchronize(s));
   t->rows.assign(t->nblk[0], 0);
   std::vector<int64_t> cnt(t->nblk[0], 0);
-  for (int64_t id : t->ids) cnt[id % t->nblk[0]]++;
+  for (int64_t id : t->ids) cnt[(id >= 0 ? id : -(id + 1)) % t->nblk[0]]++;  // marked ids are -(id)-1
   int64_t acc = 0;
   for (int r = 0; r < t->nblk[0]; ++r) { t->rows[r] = acc; acc += cnt[r]; }
   t->host_stale = false;
