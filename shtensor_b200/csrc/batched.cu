@@ -1,0 +1,329 @@
+// batched.cu -- the batched FP64 form: one persistent kernel over a size-class work list.
+//
+// Every C block is put in a size class by its matrix extents (m, n); each class has a tile
+// shape (picked by the autotuner, or by a padded-area model until tuned).  The plan builds a
+// single work list of (C block, tile, shape) items ordered by estimated cost, heaviest first;
+// a persistent grid of 128-thread CTAs (SMs x resident CTAs) pulls items from an atomic
+// counter and runs the pipelined tile (tile_pipe.cuh) of the item's shape.  Execute is a
+// counter reset plus one launch, and is what sht_plan_execute_graph captures.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <fstream>
+#include <numeric>
+#include <sstream>
+
+#include "contract.h"
+#include "device_common.cuh"
+#include "tile_pipe.cuh"
+
+namespace sht {
+
+using B0 = PipeCfg<64, 64, 8, 4>;
+using B1 = PipeCfg<128, 32, 8, 4>;
+using B2 = PipeCfg<32, 128, 4, 8>;
+using B3 = PipeCfg<128, 16, 4, 4>;
+using B4 = PipeCfg<16, 128, 4, 4>;
+using B5 = PipeCfg<32, 32, 2, 4>;
+constexpr int kNumB = 6;
+static const int kBTM[kNumB] = {64, 128, 32, 128, 16, 32};
+static const int kBTN[kNumB] = {64, 32, 128, 16, 128, 32};
+
+constexpr size_t smax(size_t a, size_t b) { return a > b ? a : b; }
+constexpr size_t kBatchedSmem =
+    smax(smax(smax(sizeof(PipeSmem<B0>), sizeof(PipeSmem<B1>)), smax(sizeof(PipeSmem<B2>), sizeof(PipeSmem<B3>))),
+         smax(sizeof(PipeSmem<B4>), sizeof(PipeSmem<B5>)));
+
+struct BatchedArgs {
+  TileMaps mp;
+  TileScalars<double> sc;
+  const double* A; const long long* offA; const int* dimsA;
+  const double* B; const long long* offB; const int* dimsB;
+  double* C; const long long* offC; const int* dimsC;
+  const int* pair_a; const int* pair_b; const int* pstart;
+  const int4* work;
+  int nwork;
+  int* counter;
+  int a_kfast, b_kfast;
+};
+
+template <class Cfg>
+__device__ __forceinline__ void run_item(const BatchedArgs& g, int4 w, unsigned char* smem) {
+  PipeSmem<Cfg>& sm = *reinterpret_cast<PipeSmem<Cfg>*>(smem);
+  const int c = w.x;
+  auto getc = [&](double*& p, const int*& d) {
+    p = g.C + g.offC[c];
+    d = g.dimsC + (long long)c * g.mp.oC;
+  };
+  auto getpair = [&](int p, const double*& a, const int*& ad, const double*& b, const int*& bd) {
+    const int ia = g.pair_a[p], ib = g.pair_b[p];
+    a = g.A + g.offA[ia];
+    ad = g.dimsA + (long long)ia * g.mp.oA;
+    b = g.B + g.offB[ib];
+    bd = g.dimsB + (long long)ib * g.mp.oB;
+  };
+  tile_run_pipe<Cfg>(g.mp, g.sc, w.y, getc, getpair, g.pstart[c], g.pstart[c + 1], g.a_kfast, g.b_kfast, sm);
+}
+
+__global__ void __launch_bounds__(128, 4) k_batched(BatchedArgs g) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  __shared__ int s_item;
+  for (;;) {
+    if (threadIdx.x == 0) s_item = atomicAdd(g.counter, 1);
+    __syncthreads();
+    const int item = s_item;
+    __syncthreads();
+    if (item >= g.nwork) break;
+    const int4 w = g.work[item];
+    switch (w.z) {
+      case 0: run_item<B0>(g, w, smem); break;
+      case 1: run_item<B1>(g, w, smem); break;
+      case 2: run_item<B2>(g, w, smem); break;
+      case 3: run_item<B3>(g, w, smem); break;
+      case 4: run_item<B4>(g, w, smem); break;
+      default: run_item<B5>(g, w, smem); break;
+    }
+  }
+}
+
+static int batched_grid(sht_ctx* ctx) {
+  static int per_sm = -1;
+  if (per_sm < 0) {
+    SHT_CUDA(cudaFuncSetAttribute(k_batched, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kBatchedSmem));
+    SHT_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_batched, 128, kBatchedSmem));
+    if (per_sm < 1) per_sm = 1;
+  }
+  return ctx->num_sms * per_sm;
+}
+
+// ------------------------------------------------------------------ size classes
+static int ilog2ceil(long long v) {
+  int b = 0;
+  while ((1LL << b) < v) ++b;
+  return b;
+}
+
+struct ClassKey {
+  int lm, ln, lk;
+  std::string str() const { return std::to_string(lm) + "," + std::to_string(ln) + "," + std::to_string(lk); }
+};
+
+// padded-area cost model: MACs the tile shape runs (padding included) + a per-tile cost
+static int model_shape(long long m, long long n) {
+  double best = 1e300;
+  int bi = 0;
+  for (int s = 0; s < kNumB; ++s) {
+    const long long tm = kBTM[s], tn = kBTN[s];
+    const long long tiles = ((m + tm - 1) / tm) * ((n + tn - 1) / tn);
+    const double cost = (double)tiles * (double)(tm * tn) + 3072.0 * (double)tiles;
+    if (cost < best) { best = cost; bi = s; }
+  }
+  return bi;
+}
+
+struct HostPlanView {
+  std::vector<long long> m, n, ksum;  // per C block
+  std::vector<int> pstart;
+  std::vector<ClassKey> key;
+};
+
+static HostPlanView host_view(sht_plan* p, cudaStream_t s) {
+  HostPlanView v;
+  sht_tensor *A = p->A, *B = p->B, *C = p->C;
+  (void)B;
+  tensor_sync_host(C, s);
+  const long long nc = p->ncblk;
+  v.pstart.resize(nc + 1);
+  SHT_CUDA(cudaMemcpyAsync(v.pstart.data(), p->d_pstart.ptr, (nc + 1) * 4, cudaMemcpyDeviceToHost, s));
+  std::vector<int> pa(p->npairs);
+  if (p->npairs) SHT_CUDA(cudaMemcpyAsync(pa.data(), p->d_pair_a.ptr, p->npairs * 4, cudaMemcpyDeviceToHost, s));
+  SHT_CUDA(cudaStreamSynchronize(s));
+  v.m.resize(nc);
+  v.n.resize(nc);
+  v.ksum.resize(nc);
+  v.key.resize(nc);
+  for (long long c = 0; c < nc; ++c) {
+    const int64_t id = C->ids[c];
+    long long m = 1, n = 1;
+    for (int ax : p->maps.rowC) m *= C->bs[ax][(id / C->gstride[ax]) % C->nblk[ax]];
+    for (int ax : p->maps.colC) n *= C->bs[ax][(id / C->gstride[ax]) % C->nblk[ax]];
+    long long ks = 0;
+    for (int q = v.pstart[c]; q < v.pstart[c + 1]; ++q) {
+      const int64_t ida = A->ids[pa[q]];
+      long long k = 1;
+      for (int ax : p->maps.colA) k *= A->bs[ax][(ida / A->gstride[ax]) % A->nblk[ax]];
+      ks += k;
+    }
+    v.m[c] = m;
+    v.n[c] = n;
+    v.ksum[c] = ks;
+    const long long kavg = (v.pstart[c + 1] > v.pstart[c]) ? ks / (v.pstart[c + 1] - v.pstart[c]) : 1;
+    v.key[c] = {ilog2ceil(m), ilog2ceil(n), ilog2ceil(std::max(1LL, kavg))};
+  }
+  return v;
+}
+
+// Work list: items (cblk, tile, shape), touched blocks sorted by cost (heaviest first), then
+// untouched blocks (beta scaling only).
+static void build_batched_work(sht_plan* p, const HostPlanView& v, const std::map<std::string, int>& shape_of,
+                               cudaStream_t s, const std::vector<char>* subset = nullptr,
+                               std::vector<int4>* out = nullptr) {
+  const long long nc = p->ncblk;
+  struct Item { int4 w; double cost; };
+  std::vector<Item> touched, untouched;
+  for (long long c = 0; c < nc; ++c) {
+    if (subset && !(*subset)[c]) continue;
+    auto it = shape_of.find(v.key[c].str());
+    const int sh = it != shape_of.end() ? it->second : model_shape(v.m[c], v.n[c]);
+    const long long tm = kBTM[sh], tn = kBTN[sh];
+    const int ntr = (int)((v.m[c] + tm - 1) / tm), ntc = (int)((v.n[c] + tn - 1) / tn);
+    const bool has = v.pstart[c + 1] > v.pstart[c];
+    const double cost = (double)tm * tn * (double)v.ksum[c] + 4096.0;
+    for (int t = 0; t < ntr * ntc; ++t) (has ? touched : untouched).push_back({make_int4((int)c, t, sh, 0), cost});
+  }
+  std::stable_sort(touched.begin(), touched.end(), [](const Item& a, const Item& b) { return a.cost > b.cost; });
+  std::vector<int4> w;
+  w.reserve(touched.size() + untouched.size());
+  for (auto& i : touched) w.push_back(i.w);
+  for (auto& i : untouched) w.push_back(i.w);
+  if (w.size() > (size_t)INT32_MAX) fail(SHT_ERR_UNSUPPORTED, "work list above 2^31 tiles");
+  if (out) {
+    *out = std::move(w);
+    return;
+  }
+  p->bwork_touched = (long long)touched.size();
+  p->bwork = (long long)w.size();
+  p->d_bwork = PoolBuf(p->ctx->pool.get(), std::max<size_t>(w.size(), 1) * sizeof(int4), s);
+  if (!w.empty()) {
+    SHT_CUDA(cudaMemcpyAsync(p->d_bwork.ptr, w.data(), w.size() * sizeof(int4), cudaMemcpyHostToDevice, s));
+    SHT_CUDA(cudaStreamSynchronize(s));
+  }
+}
+
+static void launch_batched(sht_plan* p, BatchedArgs& b, cudaStream_t s) {
+  if (b.nwork <= 0) return;
+  SHT_CUDA(cudaMemsetAsync(b.counter, 0, sizeof(int), s));
+  const int grid = std::min<long long>(batched_grid(p->ctx), b.nwork);
+  k_batched<<<grid, 128, kBatchedSmem, s>>>(b);
+  SHT_CUDA(cudaGetLastError());
+}
+
+void batched_prepare(sht_plan* p, cudaStream_t s) {
+  p->d_counter = PoolBuf(p->ctx->pool.get(), 256, s);
+  const HostPlanView v = host_view(p, s);
+  build_batched_work(p, v, p->ctx->tuned, s);
+}
+
+
+// An operand is gathered k-fast when its memory-fastest mode (mode 0) is a contracted mode.
+static int kfast_of(const std::vector<int>& contracted_modes) {
+  return std::find(contracted_modes.begin(), contracted_modes.end(), 0) != contracted_modes.end() ? 1 : 0;
+}
+
+void batched_execute(sht_plan* p, const SparseArgs& g, long long, cudaStream_t s) {
+  BatchedArgs b{};
+  b.mp = g.mp;
+  b.sc = g.sc;
+  b.A = g.A; b.offA = g.offA; b.dimsA = g.dimsA;
+  b.B = g.B; b.offB = g.offB; b.dimsB = g.dimsB;
+  b.C = g.C; b.offC = g.offC; b.dimsC = g.dimsC;
+  b.pair_a = g.pair_a; b.pair_b = g.pair_b; b.pstart = g.pstart;
+  b.work = p->d_bwork.as<int4>();
+  uint64_t one, bb;
+  const double d1 = 1.0;
+  std::memcpy(&one, &d1, 8);
+  std::memcpy(&bb, &g.sc.beta, 8);
+  b.nwork = (int)((bb == one) ? p->bwork_touched : p->bwork);
+  b.counter = p->d_counter.as<int>();
+  b.a_kfast = kfast_of(p->maps.colA);
+  b.b_kfast = kfast_of(p->maps.rowB);
+  launch_batched(p, b, s);
+}
+
+// ------------------------------------------------------------------ autotuner
+// For every size class with work, time each tile shape on a sample of the class's C blocks
+// (written to a scratch copy, never to C) and keep the fastest.  Choices persist in the
+// context and, when a file is given, in a "key shape" text file keyed by GPU name.
+void autotune(sht_plan* p, const char* cache_file, cudaStream_t s) {
+  sht_ctx* ctx = p->ctx;
+  cudaDeviceProp prop;
+  SHT_CUDA(cudaGetDeviceProperties(&prop, ctx->device));
+  std::string gpu = prop.name;
+  std::replace(gpu.begin(), gpu.end(), ' ', '_');
+  if (cache_file) {
+    std::ifstream in(cache_file);
+    std::string g, k;
+    int sh;
+    while (in >> g >> k >> sh)
+      if (g == gpu && sh >= 0 && sh < kNumB) ctx->tuned[k] = sh;
+  }
+  const HostPlanView v = host_view(p, s);
+  std::map<std::string, std::vector<long long>> members;
+  for (long long c = 0; c < p->ncblk; ++c)
+    if (v.pstart[c + 1] > v.pstart[c]) members[v.key[c].str()].push_back(c);
+  DevicePool* pool = ctx->pool.get();
+  // scratch C: offsets remapped into a compact buffer for the sampled blocks
+  std::vector<long long> offs(p->ncblk, 0);
+  cudaEvent_t e0, e1;
+  SHT_CUDA(cudaEventCreate(&e0));
+  SHT_CUDA(cudaEventCreate(&e1));
+  bool changed = false;
+  for (auto& kv : members) {
+    if (ctx->tuned.count(kv.first)) continue;
+    std::vector<char> subset(p->ncblk, 0);
+    long long elems = 0;
+    size_t taken = 0;
+    const size_t stride = std::max<size_t>(1, kv.second.size() / 256);
+    for (size_t i = 0; i < kv.second.size() && taken < 256; i += stride, ++taken) {
+      const long long c = kv.second[i];
+      subset[c] = 1;
+      offs[c] = elems;
+      elems += v.m[c] * v.n[c];
+    }
+    PoolBuf scratch(pool, std::max(elems, 1LL) * 8, s), doffs(pool, p->ncblk * 8, s), work(pool, 1, s);
+    SHT_CUDA(cudaMemcpyAsync(doffs.ptr, offs.data(), p->ncblk * 8, cudaMemcpyHostToDevice, s));
+    double best = 1e300;
+    int best_sh = model_shape(v.m[kv.second[0]], v.n[kv.second[0]]);
+    for (int sh = 0; sh < kNumB; ++sh) {
+      std::map<std::string, int> forced{{kv.first, sh}};
+      std::vector<int4> items;
+      build_batched_work(p, v, forced, s, &subset, &items);
+      work = PoolBuf(pool, items.size() * sizeof(int4), s);
+      SHT_CUDA(cudaMemcpyAsync(work.ptr, items.data(), items.size() * sizeof(int4), cudaMemcpyHostToDevice, s));
+      BatchedArgs b{};
+      b.mp = p->tmaps;
+      b.sc = {1.0, 0.0, 1, 0};
+      b.A = p->A->d_data.as<double>(); b.offA = p->A->d_offsets.as<long long>(); b.dimsA = p->A->d_dims.as<int>();
+      b.B = p->B->d_data.as<double>(); b.offB = p->B->d_offsets.as<long long>(); b.dimsB = p->B->d_dims.as<int>();
+      b.C = scratch.as<double>(); b.offC = doffs.as<long long>(); b.dimsC = p->C->d_dims.as<int>();
+      b.pair_a = p->d_pair_a.as<int>(); b.pair_b = p->d_pair_b.as<int>(); b.pstart = p->d_pstart.as<int>();
+      b.work = work.as<int4>();
+      b.nwork = (int)items.size();
+      b.counter = p->d_counter.as<int>();
+      b.a_kfast = kfast_of(p->maps.colA);
+      b.b_kfast = kfast_of(p->maps.rowB);
+      launch_batched(p, b, s);  // warm-up
+      float ms = 0, tot = 0;
+      for (int r = 0; r < 3; ++r) {
+        SHT_CUDA(cudaEventRecord(e0, s));
+        launch_batched(p, b, s);
+        SHT_CUDA(cudaEventRecord(e1, s));
+        SHT_CUDA(cudaEventSynchronize(e1));
+        SHT_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+        tot += ms;
+      }
+      if (tot < best) { best = tot; best_sh = sh; }
+    }
+    ctx->tuned[kv.first] = best_sh;
+    changed = true;
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (cache_file && changed) {
+    std::ofstream out(cache_file, std::ios::app);
+    for (auto& kv : ctx->tuned) out << gpu << " " << kv.first << " " << kv.second << "\n";
+  }
+  build_batched_work(p, v, ctx->tuned, s);
+}
+
+}  // namespace sht

@@ -460,7 +460,8 @@ sht_status sht_tensor_compare(sht_tensor* X, sht_tensor* Ref, double* max_abs, d
 sht_status sht_autotune(sht_plan* p, const char* cache_file, void* stream) {
   return guard([&] {
     need(p, "null plan");
-    (void)cache_file; (void)stream;
+    if (p->mode != SHT_MODE_BATCHED_FP64) fail(SHT_ERR_STATE, "autotune applies to batched plans");
+    autotune(p, cache_file, as_stream(stream));
   });
 }
 

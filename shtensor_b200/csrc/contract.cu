@@ -179,16 +179,6 @@ __global__ void k_tile_emit(long long nc, const long long* __restrict__ cnt_t, c
 // ---------------------------------------------------------------------------------------
 // execute kernels
 // ---------------------------------------------------------------------------------------
-struct SparseArgs {
-  TileMaps mp;
-  TileScalars<double> sc;
-  const double* A; const long long* offA; const int* dimsA;
-  const double* B; const long long* offB; const int* dimsB;
-  double* C; const long long* offC; const int* dimsC;
-  const int* pair_a; const int* pair_b; const int* pstart;
-  const int2* work;
-};
-
 template <class Cfg>
 __global__ void __launch_bounds__(Cfg::kThreads) k_contract_tiles(SparseArgs g) {
   __shared__ TileSmem<double, Cfg> sm;
@@ -576,12 +566,6 @@ void plan_execute(sht_plan* p, double alpha, double beta, cudaStream_t s) {
   } else {
     launch_tiles(p->shape, nwork, g, s);
   }
-}
-
-// Until the persistent path is tuned it launches the plain tiles.
-void batched_prepare(sht_plan*, cudaStream_t) {}
-void batched_execute(sht_plan* p, const SparseArgs& g, long long nwork, cudaStream_t s) {
-  launch_tiles(p->shape, nwork, g, s);
 }
 
 }  // namespace sht

@@ -37,14 +37,13 @@ struct sht_plan {
 
 namespace sht {
 
-struct SparseArgs;
-
 sht_plan* plan_create(sht_ctx* ctx, const std::string& expr, sht_tensor* A, sht_tensor* B, sht_tensor* C,
                       double eps, sht_norm norm, sht_mode mode, cudaStream_t s);
 void build_work(sht_plan* p, int TM, int TN, cudaStream_t s);
 void plan_execute(sht_plan* p, double alpha, double beta, cudaStream_t s);
 void batched_prepare(sht_plan* p, cudaStream_t s);
 void batched_execute(sht_plan* p, const SparseArgs& g, long long nwork_plain, cudaStream_t s);
+void autotune(sht_plan* p, const char* cache_file, cudaStream_t s);
 void block_dims_sizes(const sht_tensor* t, const long long* ids, long long n, int* dims, long long* sizes,
                       cudaStream_t s);
 void tensor_compress_device(sht_tensor* t, cudaStream_t s);

@@ -95,8 +95,12 @@ struct PoolBuf {
     return *this;
   }
   ~PoolBuf() { release(); }
-  void release() {
-    if (ptr && pool) pool->free(ptr, stream);
+  void release() noexcept {
+    // runs in destructors: a failing free (lost CUDA context) leaks instead of terminating
+    try {
+      if (ptr && pool) pool->free(ptr, stream);
+    } catch (...) {
+    }
     ptr = nullptr;
     bytes = 0;
   }

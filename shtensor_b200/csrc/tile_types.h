@@ -1,6 +1,8 @@
 // tile_types.h -- plain descriptors shared by host code and the tile kernels.
 #pragma once
 
+#include <cuda_runtime.h>
+
 #include "sht_internal.h"
 
 namespace sht {
@@ -22,6 +24,17 @@ struct TileScalars {
   T alpha, beta;
   int beta_zero;   // beta is +0.0: C is not read
   int alpha_zero;  // alpha is +0.0: products skipped
+};
+
+// Device pointers and scalars of one block-sparse execute (plain and batched forms).
+struct SparseArgs {
+  TileMaps mp;
+  TileScalars<double> sc;
+  const double* A; const long long* offA; const int* dimsA;
+  const double* B; const long long* offB; const int* dimsB;
+  double* C; const long long* offC; const int* dimsC;
+  const int* pair_a; const int* pair_b; const int* pstart;
+  const int2* work;
 };
 
 }  // namespace sht

@@ -169,3 +169,30 @@ def test_contract_errors(ctx):
     assert ei.value.status == sht.Status.ERR_PARSE
     with pytest.raises(sht.ShtError):
         sht.contract(ctx, w.expr, 1.0, A, B, 0.0, A)
+
+
+def test_autotune_keeps_results_bit_exact(ctx):
+    w = W.c1(seed=8, scale=0.35, occupancy=0.35)
+    A, B, C = dev(ctx, w.A), dev(ctx, w.B), dev(ctx, w.C)
+    plan = sht.Plan(ctx, w.expr, A, B, C, mode=sht.Mode.BATCHED_FP64)
+    plan.autotune()
+    plan.execute(1.0, 0.0)
+    want = oracle.contract(w.expr, 1.0, host(w.A), host(w.B), 0.0, host(w.C))
+    assert np.array_equal(C.download(), want.C.data)
+    assert np.array_equal(plan.pairs(), want.pairs)
+
+
+@pytest.mark.parametrize("expr,perm", [("ijl, lk -> kji", None), ("lij, kl -> ikj", None)])
+def test_permuted_layouts_bit_exact(ctx, expr, perm):
+    # contracted mode first in A (k-fast gathers) and permuted output modes
+    rng = np.random.default_rng(21)
+    sizes = {c: list(map(int, rng.integers(3, 12, 5))) for c in "ijkl"}
+    ta, tb, tc = expr.replace(" ", "").replace("->", ",").split(",")
+    A = W.build_tensor(rng, [sizes[c] for c in ta], lambda c: rng.random(len(c[0])) < 0.4, None, "normal")
+    B = W.build_tensor(rng, [sizes[c] for c in tb], lambda c: rng.random(len(c[0])) < 0.4, None, "normal")
+    wl = W.Workload("perm", expr, A, B, W.empty_tensor([sizes[c] for c in tc]))
+    for mode in MODES:
+        pairs, ids, offs, data, want, _ = run_both(ctx, wl, mode, alpha=-1.5)
+        assert np.array_equal(pairs, want.pairs)
+        assert np.array_equal(ids, want.C.ids)
+        assert np.array_equal(data, want.C.data)
