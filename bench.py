@@ -47,6 +47,9 @@ def parse():
     ap.add_argument("--cpu-sample-seconds", type=float, default=15.0)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-count", action="store_true", help="skip the CUPTI launch count (use under ncu)")
+    ap.add_argument("--no-autotune", action="store_true")
+    ap.add_argument("--pool-gb", type=float, default=60.0)
     return ap.parse_args()
 
 
@@ -215,7 +218,7 @@ def run_ours(args):
         torch.cuda.set_device(0)
     dev = torch.cuda.current_device()
     w = build_workload(args)
-    ctx = sht.Context(60 << 30, device=dev)
+    ctx = sht.Context(int(args.pool_gb * (1 << 30)), device=dev)
     stream = torch.cuda.current_stream()
 
     def T(h):
@@ -246,7 +249,7 @@ def run_ours(args):
     for fname in [f for f in args.forms.split(",") if f]:
         mode = forms[fname]
         rep = None
-        if fname == "batched":
+        if fname == "batched" and not args.no_autotune:
             tuner = sht.Plan(ctx, w.expr, A, B, Cd, mode=mode, stream=stream)
             tuner.autotune(stream=stream)
             tuner.close()
@@ -283,8 +286,8 @@ def run_ours(args):
     torch.cuda.synchronize()
     kern_ms = float(np.mean([a.elapsed_time(b) for a, b in ev]))
     prep = plan.report()
-    launches, names = count_launches(lambda: sht.contract(ctx, w.expr, 1.0, A, B, 0.0, Cd, mode=forms[best],
-                                                          stream=stream))
+    launches, names = (None, []) if args.no_count else count_launches(
+        lambda: sht.contract(ctx, w.expr, 1.0, A, B, 0.0, Cd, mode=forms[best], stream=stream))
     peak = measure_fp64_peak(sht, ctx)
     achieved = prep["flops"] / kern_ms / 1e9  # TFLOP/s
     roofline = {"bound": "tensor", "pipe": "fp64 (DFMA; B200's FP64 and FP64-tensor peaks are the same figure)",

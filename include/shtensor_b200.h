@@ -6,6 +6,8 @@
  * calling thread is returned by sht_last_error().  Handles are opaque.  Device memory for
  * tensors, plans and scratch comes from the context's device pool.  A context and the
  * handles made from it are not thread-safe: one host thread drives a context at a time.
+ * After sht_finalize the only valid calls on tensors and plans made from the context are
+ * their destroy calls; the device arena is released when the last of them is destroyed.
  * Stream arguments are cudaStream_t values passed as void* (NULL = the legacy default stream).
  *
  * Reference interfaces each entry point replaces (paths relative to the shtensor root):

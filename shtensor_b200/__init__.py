@@ -251,7 +251,7 @@ class Tensor:
     """Tensor<T,N>: block-sparse tensor resident in device memory."""
 
     def __init__(self, ctx: Context, block_sizes, dtype=np.float64):
-        self.ctx = ctx
+        self.ctx = ctx  # keeps the context (and its device arena) alive while the tensor lives
         self.block_sizes = [list(map(int, b)) for b in block_sizes]
         self.dtype = np.dtype(dtype)
         nb, pnb = _iarr([len(b) for b in self.block_sizes])

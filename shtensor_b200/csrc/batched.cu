@@ -19,20 +19,18 @@
 
 namespace sht {
 
+// tile shapes (all 128 threads); few, so the persistent kernel's code stays in cache
 using B0 = PipeCfg<64, 64, 8, 4>;
 using B1 = PipeCfg<128, 32, 8, 4>;
 using B2 = PipeCfg<32, 128, 4, 8>;
 using B3 = PipeCfg<128, 16, 4, 4>;
-using B4 = PipeCfg<16, 128, 4, 4>;
-using B5 = PipeCfg<32, 32, 2, 4>;
-constexpr int kNumB = 6;
-static const int kBTM[kNumB] = {64, 128, 32, 128, 16, 32};
-static const int kBTN[kNumB] = {64, 32, 128, 16, 128, 32};
+constexpr int kNumB = 4;
+static const int kBTM[kNumB] = {64, 128, 32, 128};
+static const int kBTN[kNumB] = {64, 32, 128, 16};
 
 constexpr size_t smax(size_t a, size_t b) { return a > b ? a : b; }
 constexpr size_t kBatchedSmem =
-    smax(smax(smax(sizeof(PipeSmem<B0>), sizeof(PipeSmem<B1>)), smax(sizeof(PipeSmem<B2>), sizeof(PipeSmem<B3>))),
-         smax(sizeof(PipeSmem<B4>), sizeof(PipeSmem<B5>)));
+    smax(smax(sizeof(PipeSmem<B0>), sizeof(PipeSmem<B1>)), smax(sizeof(PipeSmem<B2>), sizeof(PipeSmem<B3>)));
 
 struct BatchedArgs {
   TileMaps mp;
@@ -79,9 +77,7 @@ __global__ void __launch_bounds__(128, 4) k_batched(BatchedArgs g) {
       case 0: run_item<B0>(g, w, smem); break;
       case 1: run_item<B1>(g, w, smem); break;
       case 2: run_item<B2>(g, w, smem); break;
-      case 3: run_item<B3>(g, w, smem); break;
-      case 4: run_item<B4>(g, w, smem); break;
-      default: run_item<B5>(g, w, smem); break;
+      default: run_item<B3>(g, w, smem); break;
     }
   }
 }

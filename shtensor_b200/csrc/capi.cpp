@@ -61,7 +61,7 @@ sht_status sht_init(sht_ctx** out, int device, size_t pool_bytes) {
     int sms = 0;
     SHT_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
     c->num_sms = sms;
-    c->pool = std::make_unique<DevicePool>(device, pool_bytes);
+    c->pool = std::make_shared<DevicePool>(device, pool_bytes);
     SHT_CUDA(cudaStreamCreateWithFlags(&c->stage_stream, cudaStreamNonBlocking));
     *out = c.release();
   });
@@ -189,6 +189,7 @@ sht_status sht_tensor_create(sht_ctx* ctx, int order, const int* nblk, const int
     if (order > kMaxOrder) fail(SHT_ERR_UNSUPPORTED, "tensor order above 8");
     need(dtype == SHT_F32 || dtype == SHT_F64, "unknown dtype");
     auto t = std::make_unique<sht_tensor>();
+    t->keep = ctx->pool;
     t->ctx = ctx;
     t->order = order;
     t->dtype = dtype;

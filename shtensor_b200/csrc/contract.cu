@@ -302,6 +302,7 @@ sht_plan* plan_create(sht_ctx* ctx, const std::string& expr, sht_tensor* A, sht_
       if (id < 0) fail(SHT_ERR_STATE, "tensor has filtered blocks that were not compressed");
   }
   auto p = std::make_unique<sht_plan>();
+  p->keep = ctx->pool;
   p->ctx = ctx;
   p->mode = mode;
   p->A = A; p->B = B; p->C = C;

@@ -5,6 +5,7 @@
 #include "tile_types.h"
 
 struct sht_plan {
+  std::shared_ptr<sht::DevicePool> keep;  // declared first: released after the buffers below
   sht_ctx* ctx = nullptr;
   sht_mode mode = SHT_MODE_PLAIN_FP64;
   sht_tensor *A = nullptr, *B = nullptr, *C = nullptr;

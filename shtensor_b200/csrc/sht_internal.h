@@ -117,7 +117,9 @@ struct PoolBuf {
 struct sht_ctx {
   int device = 0;
   int num_sms = 148;
-  std::unique_ptr<sht::DevicePool> pool;
+  // shared with every tensor and plan: the arena outlives sht_finalize until the last
+  // handle made from the context is destroyed
+  std::shared_ptr<sht::DevicePool> pool;
   cudaStream_t stage_stream = nullptr;  // host-staging copies
   std::map<std::string, int> tuned;     // autotuner choices: size-class key -> tile id
 };
@@ -139,6 +141,7 @@ struct sht_kernel {
 };
 
 struct sht_tensor {
+  std::shared_ptr<sht::DevicePool> keep;  // declared first: released after the buffers below
   sht_ctx* ctx = nullptr;
   int order = 0;
   sht_dtype dtype = SHT_F64;

@@ -25,7 +25,7 @@ template <int TM, int TN, int TK, int RM, int RN>
 struct TileCfg {
   static constexpr int kTM = TM, kTN = TN, kTK = TK, kRM = RM, kRN = RN;
   static constexpr int kThreads = (TM / RM) * (TN / RN);
-  static constexpr int kPad = 2;
+  static constexpr int kPad = 8;
 };
 
 template <typename T, class Cfg>
@@ -63,7 +63,7 @@ __device__ __forceinline__ void tile_run(const TileMaps& mp, const TileScalars<T
                                          TileSmem<T, Cfg>& sm) {
   constexpr int TM = Cfg::kTM, TN = Cfg::kTN, TK = Cfg::kTK, RM = Cfg::kRM, RN = Cfg::kRN;
   constexpr int NT = Cfg::kThreads;
-  constexpr int XT = TM / RM;  // threads along rows
+  constexpr int XT = TM / RM, YT = TN / RN;  // threads along rows / columns
   const int tid = threadIdx.x;
   const int tx = tid % XT, ty = tid / XT;
 
@@ -121,7 +121,7 @@ __device__ __forceinline__ void tile_run(const TileMaps& mp, const TileScalars<T
 #pragma unroll
     for (int i = 0; i < RM; ++i)
 #pragma unroll
-      for (int j = 0; j < RN; ++j) acc[i][j] = mul_rn(sc.beta, sm.u.c[ty * RN + j][tx * RM + i]);
+      for (int j = 0; j < RN; ++j) acc[i][j] = mul_rn(sc.beta, sm.u.c[ty + j * YT][tx + i * XT]);
     __syncthreads();
   }
 
@@ -181,9 +181,9 @@ __device__ __forceinline__ void tile_run(const TileMaps& mp, const TileScalars<T
           for (int k = 0; k < TK; ++k) {
             T a[RM], b[RN];
 #pragma unroll
-            for (int i = 0; i < RM; ++i) a[i] = sm.u.ab.a[k][tx * RM + i];
+            for (int i = 0; i < RM; ++i) a[i] = sm.u.ab.a[k][tx + i * XT];
 #pragma unroll
-            for (int j = 0; j < RN; ++j) b[j] = sm.u.ab.b[k][ty * RN + j];
+            for (int j = 0; j < RN; ++j) b[j] = sm.u.ab.b[k][ty + j * YT];
 #pragma unroll
             for (int i = 0; i < RM; ++i)
 #pragma unroll
@@ -193,9 +193,9 @@ __device__ __forceinline__ void tile_run(const TileMaps& mp, const TileScalars<T
           for (int k = 0; k < kc; ++k) {
             T a[RM], b[RN];
 #pragma unroll
-            for (int i = 0; i < RM; ++i) a[i] = sm.u.ab.a[k][tx * RM + i];
+            for (int i = 0; i < RM; ++i) a[i] = sm.u.ab.a[k][tx + i * XT];
 #pragma unroll
-            for (int j = 0; j < RN; ++j) b[j] = sm.u.ab.b[k][ty * RN + j];
+            for (int j = 0; j < RN; ++j) b[j] = sm.u.ab.b[k][ty + j * YT];
 #pragma unroll
             for (int i = 0; i < RM; ++i)
 #pragma unroll
@@ -211,7 +211,7 @@ __device__ __forceinline__ void tile_run(const TileMaps& mp, const TileScalars<T
 #pragma unroll
   for (int i = 0; i < RM; ++i)
 #pragma unroll
-    for (int j = 0; j < RN; ++j) sm.u.c[ty * RN + j][tx * RM + i] = acc[i][j];
+    for (int j = 0; j < RN; ++j) sm.u.c[ty + j * YT][tx + i * XT] = acc[i][j];
   __syncthreads();
   for (int e = tid; e < TM * TN; e += NT) {
     const int i = e % TM, j = e / TM;

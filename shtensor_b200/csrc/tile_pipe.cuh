@@ -18,7 +18,7 @@ template <int TM_, int TN_, int RM_, int RN_>
 struct PipeCfg {
   static constexpr int TM = TM_, TN = TN_, TK = 16, RM = RM_, RN = RN_;
   static constexpr int NT = (TM / RM) * (TN / RN);
-  static constexpr int P = 2;
+  static constexpr int P = 8;  // row pitch = TM+8 doubles: staging stores hit 2 wavefronts
   static constexpr int LA = TM * TK / NT;  // A elements loaded per thread per chunk
   static constexpr int LB = TN * TK / NT;
   static_assert(NT == 128, "pipelined tiles run 128 threads");
@@ -161,35 +161,23 @@ __device__ __forceinline__ void chunk_scale(PipeSmem<Cfg>& sm, int buf, int a_kf
   }
 }
 
-template <class Cfg, int KC>
+// Thread (tx, ty) owns rows tx + i*XT and columns ty + j*YT: a warp's operand reads are
+// consecutive doubles (one wavefront per load, no bank conflicts).
+template <class Cfg>
 __device__ __forceinline__ void chunk_mma(const PipeSmem<Cfg>& sm, int buf, int kc, int tx, int ty,
                                           double (&acc)[Cfg::RM][Cfg::RN]) {
-  constexpr int RM = Cfg::RM, RN = Cfg::RN;
-  if (KC > 0) {
+  constexpr int RM = Cfg::RM, RN = Cfg::RN, XT = Cfg::TM / RM, YT = Cfg::TN / RN;
+#pragma unroll 4
+  for (int k = 0; k < kc; ++k) {
+    double a[RM], b[RN];
 #pragma unroll
-    for (int k = 0; k < KC; ++k) {
-      double a[RM], b[RN];
+    for (int i = 0; i < RM; ++i) a[i] = sm.u.ab.a[buf][k][tx + i * XT];
 #pragma unroll
-      for (int i = 0; i < RM; ++i) a[i] = sm.u.ab.a[buf][k][tx * RM + i];
+    for (int j = 0; j < RN; ++j) b[j] = sm.u.ab.b[buf][k][ty + j * YT];
 #pragma unroll
-      for (int j = 0; j < RN; ++j) b[j] = sm.u.ab.b[buf][k][ty * RN + j];
+    for (int i = 0; i < RM; ++i)
 #pragma unroll
-      for (int i = 0; i < RM; ++i)
-#pragma unroll
-        for (int j = 0; j < RN; ++j) acc[i][j] = fma(a[i], b[j], acc[i][j]);
-    }
-  } else {
-    for (int k = 0; k < kc; ++k) {
-      double a[RM], b[RN];
-#pragma unroll
-      for (int i = 0; i < RM; ++i) a[i] = sm.u.ab.a[buf][k][tx * RM + i];
-#pragma unroll
-      for (int j = 0; j < RN; ++j) b[j] = sm.u.ab.b[buf][k][ty * RN + j];
-#pragma unroll
-      for (int i = 0; i < RM; ++i)
-#pragma unroll
-        for (int j = 0; j < RN; ++j) acc[i][j] = fma(a[i], b[j], acc[i][j]);
-    }
+      for (int j = 0; j < RN; ++j) acc[i][j] = fma(a[i], b[j], acc[i][j]);
   }
 }
 
@@ -199,7 +187,7 @@ __device__ __forceinline__ void tile_run_pipe(const TileMaps& mp, const TileScal
                                               GetC getc, GetPair getpair, int pb, int pe, int a_kfast,
                                               int b_kfast, PipeSmem<Cfg>& sm) {
   constexpr int TM = Cfg::TM, TN = Cfg::TN, TK = Cfg::TK, RM = Cfg::RM, RN = Cfg::RN, NT = Cfg::NT;
-  constexpr int XT = TM / RM;
+  constexpr int XT = TM / RM, YT = TN / RN;
   const int tid = threadIdx.x;
   const int tx = tid % XT, ty = tid / XT;
 
@@ -256,7 +244,7 @@ __device__ __forceinline__ void tile_run_pipe(const TileMaps& mp, const TileScal
 #pragma unroll
     for (int i = 0; i < RM; ++i)
 #pragma unroll
-      for (int j = 0; j < RN; ++j) acc[i][j] = mul_rn(sc.beta, sm.u.c[ty * RN + j][tx * RM + i]);
+      for (int j = 0; j < RN; ++j) acc[i][j] = mul_rn(sc.beta, sm.u.c[ty + j * YT][tx + i * XT]);
     __syncthreads();
   }
 
@@ -282,11 +270,7 @@ __device__ __forceinline__ void tile_run_pipe(const TileMaps& mp, const TileScal
       // 1. chunk c+1 into the other operand buffer, asynchronously (tables in slot^1)
       chunk_issue<Cfg>(nxt, sm, slot ^ 1, slot ^ 1, mt, nt, a_kfast, b_kfast, dummy);
       // 2. multiply chunk c
-      const int kc = min(TK, cur.K - cur.k0);
-      if (kc == TK)
-        chunk_mma<Cfg, TK>(sm, slot, kc, tx, ty, acc);
-      else
-        chunk_mma<Cfg, 0>(sm, slot, kc, tx, ty, acc);
+      chunk_mma<Cfg>(sm, slot, min(TK, cur.K - cur.k0), tx, ty, acc);
       // 3. tables of chunk c+2 into slot (free: chunk c's copies were issued last iteration)
       chunk_tables<Cfg>(far, mp, sm, slot, mt, nt);
       // 4. wait for chunk c+1, scale its A by alpha
@@ -303,7 +287,7 @@ __device__ __forceinline__ void tile_run_pipe(const TileMaps& mp, const TileScal
 #pragma unroll
   for (int i = 0; i < RM; ++i)
 #pragma unroll
-    for (int j = 0; j < RN; ++j) sm.u.c[ty * RN + j][tx * RM + i] = acc[i][j];
+    for (int j = 0; j < RN; ++j) sm.u.c[ty + j * YT][tx + i * XT] = acc[i][j];
   __syncthreads();
   for (int e = tid; e < TM * TN; e += NT) {
     const int i = e % TM, j = e / TM;

@@ -107,3 +107,17 @@ def test_pool_accounting_follows_reference_spec():
         assert ei.value.status == sht.Status.ERR_OOM
         c.free(u)
         assert c.get_free_mem() == pool_memory - H
+
+
+def test_handles_outlive_finalize():
+    # destroying tensors and plans after the context was finalised must be safe
+    w = W.c0(seed=3, nblocks=4, p=0.5)
+    c = sht.Context(1 << 28)
+    A = sht.Tensor(c, w.A.block_sizes).reserve(w.A.index_lists()).upload(w.A.data)
+    B = sht.Tensor(c, w.B.block_sizes).reserve(w.B.index_lists()).upload(w.B.data)
+    C = sht.Tensor(c, w.C.block_sizes).reserve([[] for _ in w.C.block_sizes])
+    plan = sht.Plan(c, w.expr, A, B, C)
+    plan.execute()
+    c.close()
+    plan.close()
+    del A, B, C
