@@ -1,5 +1,6 @@
 // batched.cu -- the batched FP64 form: one persistent kernel over a size-class work list.
 //
+// Products run on the FP64 tensor cores (mma.sync m8n8k4, bit-identical to the fma chain).
 // Every C block is put in a size class by its matrix extents (m, n); each class has a tile
 // shape (picked by the autotuner, or by a padded-area model until tuned).  The plan builds a
 // single work list of (C block, tile, shape) items ordered by estimated cost, heaviest first;
@@ -20,10 +21,10 @@
 namespace sht {
 
 // tile shapes (all 128 threads); few, so the persistent kernel's code stays in cache
-using B0 = PipeCfg<64, 64, 8, 4>;
-using B1 = PipeCfg<128, 32, 8, 4>;
-using B2 = PipeCfg<32, 128, 4, 8>;
-using B3 = PipeCfg<128, 16, 4, 4>;
+using B0 = PipeCfg<64, 64, 2>;   // 2x2 warps of 32x32
+using B1 = PipeCfg<128, 32, 4>;  // 4x1 warps of 32x32
+using B2 = PipeCfg<32, 128, 1>;  // 1x4 warps of 32x32
+using B3 = PipeCfg<128, 16, 4>;  // 4x1 warps of 32x16
 constexpr int kNumB = 4;
 static const int kBTM[kNumB] = {64, 128, 32, 128};
 static const int kBTN[kNumB] = {64, 32, 128, 16};

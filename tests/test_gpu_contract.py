@@ -10,6 +10,7 @@ import pytest
 
 import oracle
 import shtensor_b200 as sht
+from tests.bits import bits_equal
 from shtensor_b200 import workloads as W
 
 pytestmark = pytest.mark.gpu
@@ -70,7 +71,7 @@ def test_golden_fixtures(ctx, name, mode):
     ids, offs, _ = C.get_sparse_info()
     assert np.array_equal(ids, d[f"{name}_cids"]) and np.array_equal(offs, d[f"{name}_coffs"])
     got = C.download()
-    assert np.array_equal(got, d[f"{name}_cdata"])
+    assert bits_equal(got, d[f"{name}_cdata"])
     ref = d[f"{name}_cdata_ref"]
     assert np.linalg.norm(got - ref) <= 1e-13 * np.linalg.norm(ref)
 
@@ -81,7 +82,7 @@ def test_c0_full_config_bit_exact(ctx, mode):
     pairs, ids, offs, data, want, rep = run_both(ctx, w, mode)
     assert np.array_equal(pairs, want.pairs)
     assert np.array_equal(ids, want.C.ids) and np.array_equal(offs, want.C.offsets)
-    assert np.array_equal(data, want.C.data)
+    assert bits_equal(data, want.C.data)
     assert rep["flops"] == pytest.approx(want.flops, rel=1e-12)
 
 
@@ -92,7 +93,7 @@ def test_c1_scaled_bit_exact(ctx, mode):
     assert len(pairs) > 10
     assert np.array_equal(pairs, want.pairs)
     assert np.array_equal(ids, want.C.ids) and np.array_equal(offs, want.C.offsets)
-    assert np.array_equal(data, want.C.data)
+    assert bits_equal(data, want.C.data)
 
 
 def test_c3_screening_bit_exact(ctx):
@@ -101,7 +102,7 @@ def test_c3_screening_bit_exact(ctx):
         pairs, ids, offs, data, want, _ = run_both(ctx, w, sht.Mode.PLAIN_FP64, eps=w.screen_eps, norm=norm)
         assert np.array_equal(pairs, want.pairs)
         assert np.array_equal(ids, want.C.ids)
-        assert np.array_equal(data, want.C.data)
+        assert bits_equal(data, want.C.data)
 
 
 def test_existing_c_union_and_beta(ctx):
@@ -114,7 +115,7 @@ def test_existing_c_union_and_beta(ctx):
     for beta in (0.0, 1.0, -0.5):
         pairs, ids, offs, data, want, _ = run_both(ctx, w, sht.Mode.PLAIN_FP64, alpha=2.0, beta=beta, Cinit=Ch)
         assert np.array_equal(ids, want.C.ids) and np.array_equal(offs, want.C.offsets)
-        assert np.array_equal(data, want.C.data), beta
+        assert bits_equal(data, want.C.data), beta
 
 
 def test_repeated_execute_accumulates(ctx):
@@ -128,8 +129,8 @@ def test_repeated_execute_accumulates(ctx):
     want = oracle.contract(w.expr, 1.0, host(w.A), host(w.B), 0.0, host(w.C))
     r2 = oracle.contract(w.expr, 1.0, host(w.A), host(w.B), 1.0, want.C)
     r3 = oracle.contract(w.expr, 1.0, host(w.A), host(w.B), 1.0, r2.C)
-    assert np.array_equal(first, want.C.data)
-    assert np.array_equal(C.download(), r3.C.data)
+    assert bits_equal(first, want.C.data)
+    assert bits_equal(C.download(), r3.C.data)
 
 
 def test_graph_replay_matches_direct(ctx):
@@ -142,7 +143,7 @@ def test_graph_replay_matches_direct(ctx):
         plan.execute(1.0, 0.0, stream=s, graph=True)
     s.synchronize()
     want = oracle.contract(w.expr, 1.0, host(w.A), host(w.B), 0.0, host(w.C))
-    assert np.array_equal(C.download(), want.C.data)
+    assert bits_equal(C.download(), want.C.data)
 
 
 def test_contract_entry_point_and_empty(ctx):
@@ -151,7 +152,7 @@ def test_contract_entry_point_and_empty(ctx):
     rep = sht.contract(ctx, w.expr, 1.0, A, B, 0.0, C)
     want = oracle.contract(w.expr, 1.0, host(w.A), host(w.B), 0.0, host(w.C))
     assert rep["npairs"] == len(want.pairs)
-    assert np.array_equal(C.download(), want.C.data)
+    assert bits_equal(C.download(), want.C.data)
     E = dev(ctx, W.empty_tensor(w.A.block_sizes))
     C2 = dev(ctx, w.C)
     rep = sht.contract(ctx, w.expr, 1.0, E, B, 0.0, C2)
@@ -178,7 +179,7 @@ def test_autotune_keeps_results_bit_exact(ctx):
     plan.autotune()
     plan.execute(1.0, 0.0)
     want = oracle.contract(w.expr, 1.0, host(w.A), host(w.B), 0.0, host(w.C))
-    assert np.array_equal(C.download(), want.C.data)
+    assert bits_equal(C.download(), want.C.data)
     assert np.array_equal(plan.pairs(), want.pairs)
 
 
@@ -195,4 +196,19 @@ def test_permuted_layouts_bit_exact(ctx, expr, perm):
         pairs, ids, offs, data, want, _ = run_both(ctx, wl, mode, alpha=-1.5)
         assert np.array_equal(pairs, want.pairs)
         assert np.array_equal(ids, want.C.ids)
-        assert np.array_equal(data, want.C.data)
+        assert bits_equal(data, want.C.data)
+
+
+@pytest.mark.parametrize("mode", MODES)
+def test_signed_zero_and_padding_preserved(ctx, mode):
+    # zero A blocks, negative beta on new (zero-filled) C blocks and contracted extents that are
+    # not multiples of 4: every bit, including the sign of zero, must match the oracle
+    rng = np.random.default_rng(5)
+    i, l, k = [3, 5, 7], [5, 6, 7], [2, 9]
+    A = W.build_tensor(rng, [i, l], lambda c: rng.random(len(c[0])) < 0.7, None, "normal")
+    A.data[: A.data.size // 2] = 0.0
+    B = W.build_tensor(rng, [l, k], lambda c: rng.random(len(c[0])) < 0.7, None, "normal")
+    wl = W.Workload("z", "il, lk -> ik", A, B, W.empty_tensor([i, k]))
+    for beta in (-1.0, -0.0, 0.5):
+        pairs, ids, offs, data, want, _ = run_both(ctx, wl, mode, alpha=1.0, beta=beta)
+        assert bits_equal(data, want.C.data), beta

@@ -9,6 +9,7 @@ import pytest
 
 import oracle
 import shtensor_b200 as sht
+from tests.bits import bits_equal
 from tests.golden import make_golden as G
 
 pytestmark = pytest.mark.gpu
@@ -31,7 +32,7 @@ def test_stack_fp64_device_bit_exact(ctx, kc, n):
     k.call(a, b, c, nops)
     torch.cuda.synchronize()
     got = c.cpu().numpy()
-    assert np.array_equal(got, kc[f"{n}_xmm"])
+    assert bits_equal(got, kc[f"{n}_xmm"])
     ref = kc[f"{n}_lapack_ref"]
     assert np.linalg.norm(got - ref) <= 1e-13 * max(np.linalg.norm(ref), 1e-300)
 
@@ -42,7 +43,7 @@ def test_stack_fp32_host_pointers_bit_exact(ctx, kc, n):
     k = sht.Kernel(ctx, expr, sa, sb, sc, al, be, sht.KernelType.LAPACK, dtype=np.float32)
     c = kc[f"{n}_c"].astype(np.float32)
     k.call(kc[f"{n}_a"].astype(np.float32), kc[f"{n}_b"].astype(np.float32), c, nops)
-    assert np.array_equal(c, kc[f"{n}_xmm32"])
+    assert bits_equal(c, kc[f"{n}_xmm32"])
 
 
 def test_stack_large_stack_and_big_blocks(ctx):
@@ -58,7 +59,7 @@ def test_stack_large_stack_and_big_blocks(ctx):
         k = sht.Kernel(ctx, expr, sa, sb, sc, 1.25, -0.5)
         dc = torch.from_numpy(c).cuda()
         k.call(torch.from_numpy(a).cuda(), torch.from_numpy(b).cuda(), dc, nops)
-        assert np.array_equal(dc.cpu().numpy(), want), expr
+        assert bits_equal(dc.cpu().numpy(), want), expr
 
 
 def test_kernel_errors(ctx):
