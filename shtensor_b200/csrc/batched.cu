@@ -36,14 +36,13 @@ constexpr size_t kBatchedSmem =
 struct BatchedArgs {
   TileMaps mp;
   TileScalars<double> sc;
-  const double* A; const long long* offA; const int* dimsA;
-  const double* B; const long long* offB; const int* dimsB;
+  const double* Am; const long long* aoff; const int* ald; const int* ak4;  // A in matrix form
+  const double* Bm; const long long* boff; const int* bld;                  // B in matrix form
   double* C; const long long* offC; const int* dimsC;
   const int* pair_a; const int* pair_b; const int* pstart;
   const int4* work;
   int nwork;
   int* counter;
-  int a_kfast, b_kfast;
 };
 
 template <class Cfg>
@@ -54,14 +53,15 @@ __device__ __forceinline__ void run_item(const BatchedArgs& g, int4 w, unsigned 
     p = g.C + g.offC[c];
     d = g.dimsC + (long long)c * g.mp.oC;
   };
-  auto getpair = [&](int p, const double*& a, const int*& ad, const double*& b, const int*& bd) {
+  auto getpair = [&](int p, PairView& v) {
     const int ia = g.pair_a[p], ib = g.pair_b[p];
-    a = g.A + g.offA[ia];
-    ad = g.dimsA + (long long)ia * g.mp.oA;
-    b = g.B + g.offB[ib];
-    bd = g.dimsB + (long long)ib * g.mp.oB;
+    v.a = g.Am + g.aoff[ia];
+    v.lda = g.ald[ia];
+    v.K4 = g.ak4[ia];
+    v.b = g.Bm + g.boff[ib];
+    v.ldb = g.bld[ib];
   };
-  tile_run_pipe<Cfg>(g.mp, g.sc, w.y, getc, getpair, g.pstart[c], g.pstart[c + 1], g.a_kfast, g.b_kfast, sm);
+  tile_run_pipe<Cfg>(g.mp, g.sc, w.y, getc, getpair, g.pstart[c], g.pstart[c + 1], sm);
 }
 
 __global__ void __launch_bounds__(128, 4) k_batched(BatchedArgs g) {
@@ -166,29 +166,33 @@ static void build_batched_work(sht_plan* p, const HostPlanView& v, const std::ma
                                cudaStream_t s, const std::vector<char>* subset = nullptr,
                                std::vector<int4>* out = nullptr) {
   const long long nc = p->ncblk;
-  struct Item { int4 w; double cost; };
-  std::vector<Item> touched, untouched;
+  // order C blocks (not tiles) by cost, heaviest first; untouched blocks last
+  struct Blk { double cost; int c, sh, tiles; bool has; };
+  std::vector<Blk> blks;
+  blks.reserve(nc);
+  size_t ntouched = 0, nall = 0;
   for (long long c = 0; c < nc; ++c) {
     if (subset && !(*subset)[c]) continue;
     auto it = shape_of.find(v.key[c].str());
     const int sh = it != shape_of.end() ? it->second : model_shape(v.m[c], v.n[c]);
     const long long tm = kBTM[sh], tn = kBTN[sh];
-    const int ntr = (int)((v.m[c] + tm - 1) / tm), ntc = (int)((v.n[c] + tn - 1) / tn);
+    const int tiles = (int)(((v.m[c] + tm - 1) / tm) * ((v.n[c] + tn - 1) / tn));
     const bool has = v.pstart[c + 1] > v.pstart[c];
-    const double cost = (double)tm * tn * (double)v.ksum[c] + 4096.0;
-    for (int t = 0; t < ntr * ntc; ++t) (has ? touched : untouched).push_back({make_int4((int)c, t, sh, 0), cost});
+    blks.push_back({has ? (double)tm * tn * (double)v.ksum[c] : -1.0, (int)c, sh, tiles, has});
+    nall += tiles;
+    if (has) ntouched += tiles;
   }
-  std::stable_sort(touched.begin(), touched.end(), [](const Item& a, const Item& b) { return a.cost > b.cost; });
+  std::stable_sort(blks.begin(), blks.end(), [](const Blk& a, const Blk& b) { return a.cost > b.cost; });
   std::vector<int4> w;
-  w.reserve(touched.size() + untouched.size());
-  for (auto& i : touched) w.push_back(i.w);
-  for (auto& i : untouched) w.push_back(i.w);
+  w.reserve(nall);
+  for (const Blk& b : blks)
+    for (int t = 0; t < b.tiles; ++t) w.push_back(make_int4(b.c, t, b.sh, 0));
   if (w.size() > (size_t)INT32_MAX) fail(SHT_ERR_UNSUPPORTED, "work list above 2^31 tiles");
   if (out) {
     *out = std::move(w);
     return;
   }
-  p->bwork_touched = (long long)touched.size();
+  p->bwork_touched = (long long)ntouched;
   p->bwork = (long long)w.size();
   p->d_bwork = PoolBuf(p->ctx->pool.get(), std::max<size_t>(w.size(), 1) * sizeof(int4), s);
   if (!w.empty()) {
@@ -207,22 +211,23 @@ static void launch_batched(sht_plan* p, BatchedArgs& b, cudaStream_t s) {
 
 void batched_prepare(sht_plan* p, cudaStream_t s) {
   p->d_counter = PoolBuf(p->ctx->pool.get(), 256, s);
+  matform_prepare(p, s);
   const HostPlanView v = host_view(p, s);
   build_batched_work(p, v, p->ctx->tuned, s);
 }
 
 
-// An operand is gathered k-fast when its memory-fastest mode (mode 0) is a contracted mode.
-static int kfast_of(const std::vector<int>& contracted_modes) {
-  return std::find(contracted_modes.begin(), contracted_modes.end(), 0) != contracted_modes.end() ? 1 : 0;
+static void fill_operands(sht_plan* p, BatchedArgs& b) {
+  b.Am = p->mf_a.as<double>(); b.aoff = p->mf_aoff.as<long long>(); b.ald = p->mf_ald.as<int>();
+  b.ak4 = p->mf_ak4.as<int>();
+  b.Bm = p->mf_b.as<double>(); b.boff = p->mf_boff.as<long long>(); b.bld = p->mf_bld.as<int>();
 }
 
 void batched_execute(sht_plan* p, const SparseArgs& g, long long, cudaStream_t s) {
   BatchedArgs b{};
   b.mp = g.mp;
   b.sc = g.sc;
-  b.A = g.A; b.offA = g.offA; b.dimsA = g.dimsA;
-  b.B = g.B; b.offB = g.offB; b.dimsB = g.dimsB;
+  fill_operands(p, b);
   b.C = g.C; b.offC = g.offC; b.dimsC = g.dimsC;
   b.pair_a = g.pair_a; b.pair_b = g.pair_b; b.pstart = g.pstart;
   b.work = p->d_bwork.as<int4>();
@@ -232,8 +237,7 @@ void batched_execute(sht_plan* p, const SparseArgs& g, long long, cudaStream_t s
   std::memcpy(&bb, &g.sc.beta, 8);
   b.nwork = (int)((bb == one) ? p->bwork_touched : p->bwork);
   b.counter = p->d_counter.as<int>();
-  b.a_kfast = kfast_of(p->maps.colA);
-  b.b_kfast = kfast_of(p->maps.rowB);
+  if (!g.sc.alpha_zero) matform_execute(p, g.sc.alpha, s);
   launch_batched(p, b, s);
 }
 
@@ -255,6 +259,7 @@ void autotune(sht_plan* p, const char* cache_file, cudaStream_t s) {
       if (g == gpu && sh >= 0 && sh < kNumB) ctx->tuned[k] = sh;
   }
   const HostPlanView v = host_view(p, s);
+  matform_execute(p, 1.0, s);  // operands in matrix form for the timing runs
   std::map<std::string, std::vector<long long>> members;
   for (long long c = 0; c < p->ncblk; ++c)
     if (v.pstart[c + 1] > v.pstart[c]) members[v.key[c].str()].push_back(c);
@@ -290,15 +295,12 @@ void autotune(sht_plan* p, const char* cache_file, cudaStream_t s) {
       BatchedArgs b{};
       b.mp = p->tmaps;
       b.sc = {1.0, 0.0, 1, 0};
-      b.A = p->A->d_data.as<double>(); b.offA = p->A->d_offsets.as<long long>(); b.dimsA = p->A->d_dims.as<int>();
-      b.B = p->B->d_data.as<double>(); b.offB = p->B->d_offsets.as<long long>(); b.dimsB = p->B->d_dims.as<int>();
+      fill_operands(p, b);
       b.C = scratch.as<double>(); b.offC = doffs.as<long long>(); b.dimsC = p->C->d_dims.as<int>();
       b.pair_a = p->d_pair_a.as<int>(); b.pair_b = p->d_pair_b.as<int>(); b.pstart = p->d_pstart.as<int>();
       b.work = work.as<int4>();
       b.nwork = (int)items.size();
       b.counter = p->d_counter.as<int>();
-      b.a_kfast = kfast_of(p->maps.colA);
-      b.b_kfast = kfast_of(p->maps.rowB);
       launch_batched(p, b, s);  // warm-up
       float ms = 0, tot = 0;
       for (int r = 0; r < 3; ++r) {

@@ -544,7 +544,9 @@ void build_work(sht_plan* p, int TM, int TN, cudaStream_t s) {
 void plan_execute(sht_plan* p, double alpha, double beta, cudaStream_t s) {
   sht_tensor *A = p->A, *B = p->B, *C = p->C;
   for (sht_tensor* t : {A, B, C}) tensor_touch(t, s);
-  for (PoolBuf* b : {&p->d_pair_a, &p->d_pair_b, &p->d_pstart, &p->d_work, &p->d_bwork, &p->d_counter}) b->use_on(s);
+  for (PoolBuf* b : {&p->d_pair_a, &p->d_pair_b, &p->d_pstart, &p->d_work, &p->d_bwork, &p->d_counter, &p->mf_a,
+                     &p->mf_b, &p->mf_aoff, &p->mf_boff, &p->mf_ald, &p->mf_bld, &p->mf_ak4})
+    b->use_on(s);
   SparseArgs g{};
   g.mp = p->tmaps;
   g.sc.alpha = alpha;

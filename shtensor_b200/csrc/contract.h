@@ -23,6 +23,12 @@ struct sht_plan {
   long long bwork = 0, bwork_touched = 0;
   int bclass_shape[8] = {0};
   int nclass = 0;
+  // matrix form of the operands (batched and split paths)
+  sht::PoolBuf mf_a, mf_b;          // A_mat / B_mat elements
+  sht::PoolBuf mf_aoff, mf_boff;    // int64 per block offsets
+  sht::PoolBuf mf_ald, mf_bld;      // int32 per block leading dimensions (even)
+  sht::PoolBuf mf_ak4;              // int32 per A block contracted extent rounded up to 4
+  long long mf_elems = 0;
   // split path
   sht::PoolBuf d_split;             // slices and scales (split mode)
   int split_slices = 0;
@@ -45,6 +51,8 @@ void plan_execute(sht_plan* p, double alpha, double beta, cudaStream_t s);
 void batched_prepare(sht_plan* p, cudaStream_t s);
 void batched_execute(sht_plan* p, const SparseArgs& g, long long nwork_plain, cudaStream_t s);
 void autotune(sht_plan* p, const char* cache_file, cudaStream_t s);
+void matform_prepare(sht_plan* p, cudaStream_t s);
+void matform_execute(sht_plan* p, double alpha, cudaStream_t s);
 void block_dims_sizes(const sht_tensor* t, const long long* ids, long long n, int* dims, long long* sizes,
                       cudaStream_t s);
 void tensor_compress_device(sht_tensor* t, cudaStream_t s);

@@ -9,11 +9,13 @@
 // length is not a multiple of 4 is padded with a = -0.0, b = +0.0: fma(-0, +0, c) == c for
 // every c, signed zeros included.
 //
-// Organisation:
+// Operands come in matrix form (matform.cu): every A block as an m_pad x K4 column-major
+// matrix with alpha applied and the K padding set to -0.0, every B block as an n_pad x K4
+// matrix (columns fastest) with +0.0 padding, m_pad/n_pad even and each block 16-byte
+// aligned.  So:
 //   * a tile's (pair, k-chunk) sequence is one stream of 16-deep chunks; chunk c+1 is copied
-//     global -> shared with cp.async while chunk c is multiplied;
-//   * operand offset tables are built two chunks ahead into double-buffered slots, so each
-//     chunk costs one __syncthreads();
+//     global -> shared with 16-byte cp.async while chunk c is multiplied (one __syncthreads()
+//     per chunk, no operand index tables);
 //   * 128 threads = 4 warps, each warp a WM x WN block of 8x8 accumulator fragments.
 #pragma once
 
@@ -30,10 +32,7 @@ struct PipeCfg {
   static constexpr int FM = WM / 8, FN = WN / 8;              // 8x8 fragments per warp
   static constexpr int PO = 8;  // operand pitch TM+8 doubles: fragment loads hit 2 wavefronts
   static constexpr int PC = 2;  // staging pitch TM+2 doubles: fragment stores hit 2 wavefronts
-  static constexpr int LA = TM * TK / NT;  // A elements copied per thread per chunk
-  static constexpr int LB = TN * TK / NT;
   static_assert(WM % 8 == 0 && WN % 8 == 0, "warp tile in 8x8 fragments");
-  static_assert((TM * TK) % NT == 0 && (TN * TK) % NT == 0, "copy split");
 };
 
 template <class Cfg>
@@ -47,139 +46,63 @@ struct PipeSmem {
     double c[TN][TM + Cfg::PC];
   } u;
   int rowC[TM], colC[TN];
-  int rowA[2][TM], colB[2][TN];
-  int kA[2][TK], kB[2][TK];
-  short rdig[kMaxOrder][TM];
-  short cdig[kMaxOrder][TN];
+};
+
+// Operand views of one pair: matrix-form bases, leading dimensions and K rounded up to 4.
+struct PairView {
+  const double* a;  // A_mat: element (row r, k) at a[k*lda + r]
+  const double* b;  // B_mat: element (k, col c) at b[k*ldb + c]
+  int lda, ldb, K4;
 };
 
 // Walks the (pair, k-chunk) sequence of one tile.  Every thread holds an identical copy.
 struct ChunkIter {
-  int p, pe, k0, K;
-  const double* a;
-  const double* b;
-  const int* ad;
-  const int* bd;
+  int p, pe, k0;
+  PairView v;
 };
 
 template <class GetPair>
-__device__ __forceinline__ void chunk_open(ChunkIter& it, const TileMaps& mp, GetPair& getpair) {
-  if (it.p < it.pe) {
-    getpair(it.p, it.a, it.ad, it.b, it.bd);
-    int K = 1;
-    for (int t = 0; t < mp.kk.n; ++t) K *= it.ad[mp.kk.x[t]];
-    it.K = K;
-  }
+__device__ __forceinline__ void chunk_open(ChunkIter& it, GetPair& getpair) {
+  if (it.p < it.pe) getpair(it.p, it.v);
 }
 
 template <class GetPair>
-__device__ __forceinline__ void chunk_next(ChunkIter& it, int TK, const TileMaps& mp, GetPair& getpair) {
+__device__ __forceinline__ void chunk_next(ChunkIter& it, int TK, GetPair& getpair) {
   it.k0 += TK;
-  if (it.k0 >= it.K) {
+  if (it.k0 >= it.v.K4) {
     it.k0 = 0;
     ++it.p;
-    chunk_open(it, mp, getpair);
+    chunk_open(it, getpair);
   }
 }
 
-// Offset tables of chunk `it` into table slot s (A rows and B columns for the pair, k offsets).
-template <class Cfg>
-__device__ __forceinline__ void chunk_tables(const ChunkIter& it, const TileMaps& mp, PipeSmem<Cfg>& sm, int s) {
-  constexpr int TM = Cfg::TM, TN = Cfg::TN, TK = Cfg::TK, NT = Cfg::NT;
-  if (it.p >= it.pe) return;
-  int stA[kMaxOrder], stB[kMaxOrder];
-  block_strides(it.ad, mp.oA, stA);
-  block_strides(it.bd, mp.oB, stB);
-  const int kc = min(TK, it.K - it.k0);
-  for (int i = threadIdx.x; i < TM + TN + TK; i += NT) {
-    if (i < TM) {
-      int off = 0;
-      for (int t = 0; t < mp.row.n; ++t) off += sm.rdig[t][i] * stA[mp.row.x[t]];
-      sm.rowA[s][i] = off;
-    } else if (i < TM + TN) {
-      const int j = i - TM;
-      int off = 0;
-      for (int t = 0; t < mp.col.n; ++t) off += sm.cdig[t][j] * stB[mp.col.x[t]];
-      sm.colB[s][j] = off;
-    } else {
-      const int k = i - TM - TN;
-      int q = it.k0 + k, oa = 0, ob = 0;
-      if (k < kc) {
-        for (int t = 0; t < mp.kk.n; ++t) {
-          const int e = it.ad[mp.kk.x[t]];
-          const int dgt = q % e;
-          q /= e;
-          oa += dgt * stA[mp.kk.x[t]];
-          ob += dgt * stB[mp.kk.y[t]];
-        }
-      }
-      sm.kA[s][k] = oa;
-      sm.kB[s][k] = ob;
-    }
-  }
-}
-
-__device__ __forceinline__ void cp_async8(void* smem, const void* gmem, int bytes) {
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem, int bytes) {
   const unsigned sa = static_cast<unsigned>(__cvta_generic_to_shared(smem));
-  asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(sa), "l"(gmem), "r"(bytes) : "memory");
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(sa), "l"(gmem), "r"(bytes) : "memory");
 }
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
 
-// Element q of this thread's share of a chunk: (row or column index, k).  Rows/columns run
-// fastest (coalesced when the operand's mode 0 is a free mode) unless kfast.
-template <int TX>
-__device__ __forceinline__ void chunk_elem(int q, int kfast, int TK, int& x, int& k) {
-  const int e = threadIdx.x + q * 128;
-  x = kfast ? e / TK : e % TX;
-  k = kfast ? e % TK : e / TX;
-}
-
-// Global -> shared (asynchronous) for chunk `it` with table slot s into operand buffer buf.
-// Out-of-range elements are zero-filled (source size 0; the source address is then a valid
-// operand base that is never read).
+// Global -> shared (asynchronous) of chunk `it` into operand buffer buf: kc4 k-rows of TM
+// A rows and TN B columns, as 16-byte pairs; pairs past the block's padded extent are
+// zero-filled (source size 0, source address the valid block base, never read).
 template <class Cfg>
-__device__ __forceinline__ void chunk_issue(const ChunkIter& it, PipeSmem<Cfg>& sm, int s, int buf, int mt, int nt,
-                                            int a_kfast, int b_kfast, const double* dummy) {
-  constexpr int TM = Cfg::TM, TN = Cfg::TN, TK = Cfg::TK;
-  const int kc = (it.p < it.pe) ? min(TK, it.K - it.k0) : 0;
-  const double* abase = kc ? it.a : dummy;
-  const double* bbase = kc ? it.b : dummy;
-#pragma unroll
-  for (int q = 0; q < Cfg::LA; ++q) {
-    int i, k;
-    chunk_elem<TM>(q, a_kfast, TK, i, k);
-    const bool ok = i < mt && k < kc;
-    cp_async8(&sm.u.ab.a[buf][k][i], ok ? abase + sm.rowA[s][i] + sm.kA[s][k] : abase, ok ? 8 : 0);
+__device__ __forceinline__ void chunk_issue(const ChunkIter& it, PipeSmem<Cfg>& sm, int buf, int r0, int c0) {
+  constexpr int TM = Cfg::TM, TN = Cfg::TN, TK = Cfg::TK, NT = Cfg::NT;
+  if (it.p >= it.pe) return;
+  const int kc4 = min(TK, it.v.K4 - it.k0);
+  constexpr int HA = TM / 2, HB = TN / 2;
+  for (int e = threadIdx.x; e < kc4 * HA; e += NT) {
+    const int k = e / HA, r = 2 * (e % HA);
+    const bool ok = r0 + r < it.v.lda;
+    const double* src = it.v.a + (long long)(it.k0 + k) * it.v.lda + (ok ? r0 + r : 0);
+    cp_async16(&sm.u.ab.a[buf][k][r], src, ok ? 16 : 0);
   }
-#pragma unroll
-  for (int q = 0; q < Cfg::LB; ++q) {
-    int j, k;
-    chunk_elem<TN>(q, b_kfast, TK, j, k);
-    const bool ok = j < nt && k < kc;
-    cp_async8(&sm.u.ab.b[buf][k][j], ok ? bbase + sm.kB[s][k] + sm.colB[s][j] : bbase, ok ? 8 : 0);
-  }
-  cp_async_commit();
-}
-
-// After this thread's copies landed: a = alpha*a on the A elements it copied (the XMM kernel
-// scales a before the fma; skipped when alpha == 1 where the product is exact), and a = -0.0
-// in the k padding up to the next multiple of 4.
-template <class Cfg>
-__device__ __forceinline__ void chunk_fix(PipeSmem<Cfg>& sm, int buf, int a_kfast, double alpha, bool scale, int kc) {
-  constexpr int TM = Cfg::TM, TK = Cfg::TK;
-  const int kc4 = (kc + 3) & ~3;
-  if (!scale && kc == kc4) return;
-#pragma unroll
-  for (int q = 0; q < Cfg::LA; ++q) {
-    int i, k;
-    chunk_elem<TM>(q, a_kfast, TK, i, k);
-    double& v = sm.u.ab.a[buf][k][i];
-    if (k < kc) {
-      if (scale) v = mul_rn(alpha, v);
-    } else if (k < kc4) {
-      v = -0.0;
-    }
+  for (int e = threadIdx.x; e < kc4 * HB; e += NT) {
+    const int k = e / HB, c = 2 * (e % HB);
+    const bool ok = c0 + c < it.v.ldb;
+    const double* src = it.v.b + (long long)(it.k0 + k) * it.v.ldb + (ok ? c0 + c : 0);
+    cp_async16(&sm.u.ab.b[buf][k][c], src, ok ? 16 : 0);
   }
 }
 
@@ -211,8 +134,7 @@ __device__ __forceinline__ void chunk_mma(const PipeSmem<Cfg>& sm, int buf, int 
 // One tile of one C block; pairs pb..pe-1.
 template <class Cfg, class GetC, class GetPair>
 __device__ __forceinline__ void tile_run_pipe(const TileMaps& mp, const TileScalars<double>& sc, int tile,
-                                              GetC getc, GetPair getpair, int pb, int pe, int a_kfast,
-                                              int b_kfast, PipeSmem<Cfg>& sm) {
+                                              GetC getc, GetPair getpair, int pb, int pe, PipeSmem<Cfg>& sm) {
   constexpr int TM = Cfg::TM, TN = Cfg::TN, TK = Cfg::TK, NT = Cfg::NT;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int wm0 = (warp % Cfg::WARPS_M) * Cfg::WM, wn0 = (warp / Cfg::WARPS_M) * Cfg::WN;
@@ -235,10 +157,8 @@ __device__ __forceinline__ void tile_run_pipe(const TileMaps& mp, const TileScal
       int r = r0 + i, off = 0;
       for (int t = 0; t < mp.row.n; ++t) {
         const int e = cd[mp.row.y[t]];
-        const int dgt = (i < mt) ? r % e : 0;
+        off += (r % e) * stC[mp.row.y[t]];
         r /= e;
-        sm.rdig[t][i] = (short)dgt;
-        off += dgt * stC[mp.row.y[t]];
       }
       sm.rowC[i] = (i < mt) ? off : 0;
     } else {
@@ -246,10 +166,8 @@ __device__ __forceinline__ void tile_run_pipe(const TileMaps& mp, const TileScal
       int c = c0 + j, off = 0;
       for (int t = 0; t < mp.col.n; ++t) {
         const int e = cd[mp.col.y[t]];
-        const int dgt = (j < nt) ? c % e : 0;
+        off += (c % e) * stC[mp.col.y[t]];
         c /= e;
-        sm.cdig[t][j] = (short)dgt;
-        off += dgt * stC[mp.col.y[t]];
       }
       sm.colC[j] = (j < nt) ? off : 0;
     }
@@ -279,36 +197,26 @@ __device__ __forceinline__ void tile_run_pipe(const TileMaps& mp, const TileScal
   }
 
   if (!sc.alpha_zero && pb < pe) {
-    const bool scale = sc.alpha != 1.0;
-    ChunkIter cur{pb, pe, 0, 0, nullptr, nullptr, nullptr, nullptr};
-    chunk_open(cur, mp, getpair);
-    const double* dummy = cur.a;
+    ChunkIter cur{pb, pe, 0, {}};
+    chunk_open(cur, getpair);
     ChunkIter nxt = cur;
-    chunk_next(nxt, TK, mp, getpair);
-    chunk_tables<Cfg>(cur, mp, sm, 0);
-    chunk_tables<Cfg>(nxt, mp, sm, 1);
-    __syncthreads();
-    chunk_issue<Cfg>(cur, sm, 0, 0, mt, nt, a_kfast, b_kfast, dummy);
+    chunk_next(nxt, TK, getpair);
+    chunk_issue<Cfg>(cur, sm, 0, r0, c0);
+    cp_async_commit();
     cp_async_wait_all();
-    chunk_fix<Cfg>(sm, 0, a_kfast, sc.alpha, scale, min(TK, cur.K - cur.k0));
     __syncthreads();
-    ChunkIter far = nxt;
-    chunk_next(far, TK, mp, getpair);
     int slot = 0;
     while (cur.p < pe) {
-      // 1. chunk c+1 into the other operand buffer, asynchronously (tables in slot^1)
-      chunk_issue<Cfg>(nxt, sm, slot ^ 1, slot ^ 1, mt, nt, a_kfast, b_kfast, dummy);
+      // 1. chunk c+1 into the other operand buffer, asynchronously
+      chunk_issue<Cfg>(nxt, sm, slot ^ 1, r0, c0);
+      cp_async_commit();
       // 2. multiply chunk c
-      chunk_mma<Cfg>(sm, slot, (min(TK, cur.K - cur.k0) + 3) & ~3, wm0, wn0, lane, acc);
-      // 3. tables of chunk c+2 into slot (its last reader, chunk c's copy issue, is done)
-      chunk_tables<Cfg>(far, mp, sm, slot);
-      // 4. wait for chunk c+1; alpha scaling and k padding of its A elements
+      chunk_mma<Cfg>(sm, slot, min(TK, cur.v.K4 - cur.k0), wm0, wn0, lane, acc);
+      // 3. chunk c+1 landed for every thread
       cp_async_wait_all();
-      if (nxt.p < pe) chunk_fix<Cfg>(sm, slot ^ 1, a_kfast, sc.alpha, scale, min(TK, nxt.K - nxt.k0));
       __syncthreads();
       cur = nxt;
-      nxt = far;
-      if (far.p < pe) chunk_next(far, TK, mp, getpair);
+      if (nxt.p < pe) chunk_next(nxt, TK, getpair);
       slot ^= 1;
     }
   }
