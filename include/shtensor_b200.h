@@ -150,6 +150,9 @@ sht_status sht_tensor_compare(sht_tensor* X, sht_tensor* Ref, double* max_abs, d
 /* sweeps tile shapes per (m,n,k) size class of the plan and stores the choice; file may be NULL */
 sht_status sht_autotune(sht_plan* p, const char* cache_file, void* stream);
 
+/* INT8 slices per operand used by SHT_MODE_SPLIT plans made after the call (1..8, default 7) */
+sht_status sht_set_split_slices(sht_ctx* ctx, int slices);
+
 /* ---- diagnostics ---- */
 /* which = 0: FP64 FMA peak of this GPU in TFLOP/s (the FP64 kernels' roofline denominator) */
 sht_status sht_measure_peak(sht_ctx* ctx, int which, double* value);

@@ -108,6 +108,7 @@ _SIGS = {
     "sht_tensor_compare": [_P, _P, C.POINTER(C.c_double), C.POINTER(C.c_double), _P],
     "sht_autotune": [_P, C.c_char_p, _P],
     "sht_measure_peak": [_P, C.c_int, C.POINTER(C.c_double)],
+    "sht_set_split_slices": [_P, C.c_int],
 }
 
 
@@ -183,6 +184,10 @@ class Context:
 
     def get_free_mem(self) -> int:
         return self.pool_info()["free"]
+
+    def set_split_slices(self, slices: int):
+        """INT8 slices per operand of split-precision plans made afterwards (1..8)."""
+        _check(lib().sht_set_split_slices(self._h, slices))
 
     def configure_pool(self, chunk_header: int, alignment: int):
         _check(lib().sht_pool_configure(self._h, chunk_header, alignment))

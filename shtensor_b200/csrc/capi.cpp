@@ -10,6 +10,11 @@ namespace sht {
 
 double measure_fp64_tflops(sht_ctx* ctx);
 
+static void prepare_mode(sht_plan* p, cudaStream_t s) {
+  if (p->mode == SHT_MODE_BATCHED_FP64) batched_prepare(p, s);
+  if (p->mode == SHT_MODE_SPLIT) split_prepare(p, p->ctx->split_slices ? p->ctx->split_slices : split_slices_default(), s);
+}
+
 static thread_local std::string g_last_error;
 
 void set_last_error(const std::string& msg) { g_last_error = msg; }
@@ -342,8 +347,9 @@ sht_status sht_plan_create(sht_ctx* ctx, const char* expr, sht_tensor* A, sht_te
     need(ctx && expr && out, "null argument");
     need(mode >= SHT_MODE_PLAIN_FP64 && mode <= SHT_MODE_SPLIT, "unknown mode");
     need(norm >= SHT_NORM_FROBENIUS && norm <= SHT_NORM_FROBENIUS_REFCOMPAT, "unknown norm");
-    *out = plan_create(ctx, expr, A, B, C, eps, norm, mode, as_stream(stream));
-    if ((*out)->mode == SHT_MODE_BATCHED_FP64) batched_prepare(*out, as_stream(stream));
+    std::unique_ptr<sht_plan> p(plan_create(ctx, expr, A, B, C, eps, norm, mode, as_stream(stream)));
+    prepare_mode(p.get(), as_stream(stream));
+    *out = p.release();
   });
 }
 
@@ -351,6 +357,8 @@ sht_status sht_plan_execute(sht_plan* p, double alpha, double beta, void* stream
   return guard([&] {
     need(p, "null plan");
     plan_execute(p, alpha, beta, as_stream(stream));
+    // split mode reports its bounded-wait and input checks synchronously
+    if (p->mode == SHT_MODE_SPLIT) split_check(p, as_stream(stream));
   });
 }
 
@@ -434,8 +442,9 @@ sht_status sht_contract(sht_ctx* ctx, const char* expr, double alpha, sht_tensor
     need(norm >= SHT_NORM_FROBENIUS && norm <= SHT_NORM_FROBENIUS_REFCOMPAT, "unknown norm");
     cudaStream_t s = as_stream(stream);
     std::unique_ptr<sht_plan> p(plan_create(ctx, expr, A, B, C, eps, norm, mode, s));
-    if (p->mode == SHT_MODE_BATCHED_FP64) batched_prepare(p.get(), s);
+    prepare_mode(p.get(), s);
     plan_execute(p.get(), alpha, beta, s);
+    if (p->mode == SHT_MODE_SPLIT) split_check(p.get(), s);
     if (rep) {
       std::memset(rep, 0, sizeof(*rep));
       rep->npairs = p->npairs;
@@ -453,8 +462,7 @@ sht_status sht_contract(sht_ctx* ctx, const char* expr, double alpha, sht_tensor
 sht_status sht_tensor_compare(sht_tensor* X, sht_tensor* Ref, double* max_abs, double* rel_fro, void* stream) {
   return guard([&] {
     need(X && Ref, "null tensor");
-    fail(SHT_ERR_UNSUPPORTED, "tensor compare is not built yet");
-    (void)max_abs; (void)rel_fro; (void)stream;
+    tensor_compare_device(X, Ref, max_abs, rel_fro, as_stream(stream));
   });
 }
 
@@ -463,6 +471,14 @@ sht_status sht_autotune(sht_plan* p, const char* cache_file, void* stream) {
     need(p, "null plan");
     if (p->mode != SHT_MODE_BATCHED_FP64) fail(SHT_ERR_STATE, "autotune applies to batched plans");
     autotune(p, cache_file, as_stream(stream));
+  });
+}
+
+sht_status sht_set_split_slices(sht_ctx* ctx, int slices) {
+  return guard([&] {
+    need(ctx, "null context");
+    if (slices < 1 || slices > 8) fail(SHT_ERR_INVALID, "split slices must be 1..8");
+    ctx->split_slices = slices;
   });
 }
 

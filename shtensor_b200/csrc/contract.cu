@@ -547,6 +547,9 @@ void plan_execute(sht_plan* p, double alpha, double beta, cudaStream_t s) {
   for (PoolBuf* b : {&p->d_pair_a, &p->d_pair_b, &p->d_pstart, &p->d_work, &p->d_bwork, &p->d_counter, &p->mf_a,
                      &p->mf_b, &p->mf_aoff, &p->mf_boff, &p->mf_ald, &p->mf_bld, &p->mf_ak4})
     b->use_on(s);
+  for (PoolBuf* b : {&p->sp_a, &p->sp_b, &p->sp_ae, &p->sp_be, &p->sp_aoff, &p->sp_boff, &p->sp_aeoff, &p->sp_beoff,
+                     &p->sp_err})
+    b->use_on(s);
   SparseArgs g{};
   g.mp = p->tmaps;
   g.sc.alpha = alpha;
@@ -566,6 +569,8 @@ void plan_execute(sht_plan* p, double alpha, double beta, cudaStream_t s) {
   const long long nwork = (bb == one) ? p->nwork_touched : p->nwork;
   if (p->mode == SHT_MODE_BATCHED_FP64) {
     batched_execute(p, g, nwork, s);
+  } else if (p->mode == SHT_MODE_SPLIT) {
+    split_execute(p, g, s);
   } else {
     launch_tiles(p->shape, nwork, g, s);
   }

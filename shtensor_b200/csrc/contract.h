@@ -29,8 +29,8 @@ struct sht_plan {
   sht::PoolBuf mf_ald, mf_bld;      // int32 per block leading dimensions (even)
   sht::PoolBuf mf_ak4;              // int32 per A block contracted extent rounded up to 4
   long long mf_elems = 0;
-  // split path
-  sht::PoolBuf d_split;             // slices and scales (split mode)
+  // split path: INT8 slices (K-major rows), row / column exponents, error words
+  sht::PoolBuf sp_a, sp_b, sp_ae, sp_be, sp_aoff, sp_boff, sp_aeoff, sp_beoff, sp_err;
   int split_slices = 0;
   // graph replay
   cudaGraph_t graph = nullptr;
@@ -52,6 +52,10 @@ void batched_prepare(sht_plan* p, cudaStream_t s);
 void batched_execute(sht_plan* p, const SparseArgs& g, long long nwork_plain, cudaStream_t s);
 void autotune(sht_plan* p, const char* cache_file, cudaStream_t s);
 void matform_prepare(sht_plan* p, cudaStream_t s);
+void split_prepare(sht_plan* p, int S, cudaStream_t s);
+void split_execute(sht_plan* p, const SparseArgs& sa, cudaStream_t s);
+void split_check(sht_plan* p, cudaStream_t s);
+int split_slices_default();
 void matform_execute(sht_plan* p, double alpha, cudaStream_t s);
 void block_dims_sizes(const sht_tensor* t, const long long* ids, long long n, int* dims, long long* sizes,
                       cudaStream_t s);

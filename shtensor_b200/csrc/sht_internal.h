@@ -122,6 +122,7 @@ struct sht_ctx {
   std::shared_ptr<sht::DevicePool> pool;
   cudaStream_t stage_stream = nullptr;  // host-staging copies
   std::map<std::string, int> tuned;     // autotuner choices: size-class key -> tile id
+  int split_slices = 0;                 // INT8 slices per operand in split mode (0 = default)
 };
 
 // Parsed einsum: matrix dimension <-> tensor modes (local positions)
@@ -177,6 +178,7 @@ void tensor_norms_device(sht_tensor* t, sht_norm norm, double* d_out, cudaStream
 // is ordered after the work queued on `s` so far.
 void tensor_touch(sht_tensor* t, cudaStream_t s);
 int64_t block_size_of(const sht_tensor* t, int64_t id);
+void tensor_compare_device(sht_tensor* X, sht_tensor* R, double* max_abs, double* rel_fro, cudaStream_t s);
 
 // stack kernel (stack.cu)
 void stack_call(sht_kernel* k, const void* a, const void* b, void* c, int64_t nb_ops,

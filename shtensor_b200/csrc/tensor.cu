@@ -9,6 +9,7 @@
 
 #include <algorithm>
 #include <cstring>
+#include <cmath>
 #include <numeric>
 
 #include "device_common.cuh"
@@ -278,6 +279,50 @@ void tensor_filter_device(sht_tensor* t, double eps, sht_norm norm, int compress
   } else {
     tensor_sync_host(t, s);
   }
+}
+
+// ---------------------------------------------------------------------------------------
+// Error of X against Ref over the same block pattern: max |x - r|, sum (x-r)^2, sum r^2.
+// ---------------------------------------------------------------------------------------
+__global__ void k_compare(const double* __restrict__ x, const double* __restrict__ r, long long n,
+                          unsigned long long* __restrict__ maxbits, double* __restrict__ sums) {
+  double mx = 0.0, d2 = 0.0, r2 = 0.0;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    const double d = x[i] - r[i];
+    mx = fmax(mx, fabs(d));
+    d2 = fma(d, d, d2);
+    r2 = fma(r[i], r[i], r2);
+  }
+  for (int off = 16; off >= 1; off >>= 1) {
+    mx = fmax(mx, __shfl_down_sync(0xffffffffu, mx, off));
+    d2 += __shfl_down_sync(0xffffffffu, d2, off);
+    r2 += __shfl_down_sync(0xffffffffu, r2, off);
+  }
+  if ((threadIdx.x & 31) == 0) {
+    atomicMax(maxbits, (unsigned long long)__double_as_longlong(mx));  // non-negative: bit order = value order
+    atomicAdd(&sums[0], d2);
+    atomicAdd(&sums[1], r2);
+  }
+}
+
+void tensor_compare_device(sht_tensor* X, sht_tensor* R, double* max_abs, double* rel_fro, cudaStream_t s) {
+  tensor_sync_host(X, s);
+  tensor_sync_host(R, s);
+  if (X->dtype != SHT_F64 || R->dtype != SHT_F64) fail(SHT_ERR_UNSUPPORTED, "compare runs on FP64 tensors");
+  if (X->ids != R->ids || X->nnz != R->nnz) fail(SHT_ERR_SIZE, "compare needs the same block pattern");
+  PoolBuf acc(X->ctx->pool.get(), 64, s);
+  SHT_CUDA(cudaMemsetAsync(acc.ptr, 0, 64, s));
+  if (X->nnz)
+    k_compare<<<grid_for(X->nnz, 256, X->ctx->num_sms * 8), 256, 0, s>>>(
+        X->d_data.as<double>(), R->d_data.as<double>(), X->nnz, acc.as<unsigned long long>(), acc.as<double>() + 1);
+  SHT_CUDA(cudaGetLastError());
+  double h[3];
+  SHT_CUDA(cudaMemcpyAsync(h, acc.ptr, 24, cudaMemcpyDeviceToHost, s));
+  SHT_CUDA(cudaStreamSynchronize(s));
+  unsigned long long bits;
+  std::memcpy(&bits, &h[0], 8);
+  if (max_abs) *max_abs = h[0];
+  if (rel_fro) *rel_fro = h[2] > 0 ? std::sqrt(h[1] / h[2]) : std::sqrt(h[1]);
 }
 
 }  // namespace sht

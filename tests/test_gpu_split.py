@@ -1,0 +1,99 @@
+"""Split-precision (Ozaki, INT8 tensor-core slices with FP64 reassembly) contraction on the
+B200 against the FP64 oracle.
+
+Bar: result pattern and pair list bit-exact; values within 1e-12 relative Frobenius of the
+oracle (the FP64-accurate target), max abs error reported."""
+import numpy as np
+import pytest
+
+import oracle
+import shtensor_b200 as sht
+from shtensor_b200 import workloads as W
+
+pytestmark = pytest.mark.gpu
+REL_TOL = 1e-12
+
+
+def dev(ctx, h):
+    t = sht.Tensor(ctx, h.block_sizes)
+    t.reserve(h.index_lists() if len(h.ids) else [[] for _ in h.block_sizes])
+    if h.nnz:
+        t.upload(h.data)
+    return t
+
+
+def host(t):
+    return oracle.HostTensor(t.block_sizes, t.ids, t.offsets, t.data)
+
+
+def run_split(ctx, w, alpha=1.0, beta=0.0, Cinit=None):
+    A, B = dev(ctx, w.A), dev(ctx, w.B)
+    Ch = Cinit if Cinit is not None else w.C
+    C = dev(ctx, Ch)
+    plan = sht.Plan(ctx, w.expr, A, B, C, w.screen_eps, sht.BlockNorm.FROBENIUS, sht.Mode.SPLIT)
+    plan.execute(alpha, beta)
+    want = oracle.contract(w.expr, alpha, host(w.A), host(w.B), beta, host(Ch), eps=w.screen_eps)
+    ids, offs, _ = C.get_sparse_info()
+    got = C.download()
+    assert np.array_equal(plan.pairs(), want.pairs)
+    assert np.array_equal(ids, want.C.ids) and np.array_equal(offs, want.C.offsets)
+    err = np.linalg.norm(got - want.C.data) / max(np.linalg.norm(want.C.data), 1e-300)
+    return err, np.abs(got - want.C.data).max(), plan.report()
+
+
+def test_split_tiny_c0(ctx):
+    err, mx, rep = run_split(ctx, W.c0(seed=2, nblocks=4, p=0.5))
+    assert rep["slices"] == 7
+    assert err <= REL_TOL, (err, mx)
+
+
+def test_split_c1_scaled(ctx):
+    err, mx, _ = run_split(ctx, W.c1(seed=3, scale=0.3, occupancy=0.4), alpha=0.5)
+    assert err <= REL_TOL, (err, mx)
+
+
+def test_split_mixed_magnitudes(ctx):
+    # per-block magnitudes 10^U(-6,2): per-row / per-column scaling keeps every pair accurate
+    err, mx, _ = run_split(ctx, W.c2(seed=4, scale=0.3, occupancy=0.4))
+    assert err <= REL_TOL, (err, mx)
+
+
+def test_split_existing_c_and_beta(ctx):
+    w = W.c0(seed=9, nblocks=6, p=0.4)
+    rng = np.random.default_rng(2)
+    grid = int(np.prod([len(b) for b in w.C.block_sizes]))
+    cid = np.sort(rng.choice(grid, 30, replace=False))
+    Ch = W.build_tensor(rng, w.C.block_sizes, lambda c: np.isin(np.arange(grid), cid), None, "normal")
+    err, mx, _ = run_split(ctx, w, alpha=2.0, beta=-0.5, Cinit=Ch)
+    assert err <= REL_TOL, (err, mx)
+
+
+def test_split_slice_count_tradeoff(ctx):
+    w = W.c1(seed=5, scale=0.25, occupancy=0.5)
+    errs = {}
+    for S in (4, 7):
+        ctx.set_split_slices(S)
+        try:
+            errs[S] = run_split(ctx, w)[0]
+        finally:
+            ctx.set_split_slices(7)
+    assert errs[7] <= REL_TOL and errs[4] > errs[7]
+
+
+def test_split_rejects_non_finite(ctx):
+    w = W.c0(seed=6, nblocks=4, p=0.6)
+    w.A.data[3] = np.inf
+    A, B, C = dev(ctx, w.A), dev(ctx, w.B), dev(ctx, w.C)
+    with pytest.raises(sht.ShtError) as ei:
+        sht.contract(ctx, w.expr, 1.0, A, B, 0.0, C, mode=sht.Mode.SPLIT)
+    assert ei.value.status == sht.Status.ERR_UNSUPPORTED
+
+
+def test_compare_entry_point(ctx):
+    w = W.c1(seed=6, scale=0.25, occupancy=0.5)
+    A, B = dev(ctx, w.A), dev(ctx, w.B)
+    C1, C2 = dev(ctx, w.C), dev(ctx, w.C)
+    sht.contract(ctx, w.expr, 1.0, A, B, 0.0, C1, mode=sht.Mode.BATCHED_FP64)
+    sht.contract(ctx, w.expr, 1.0, A, B, 0.0, C2, mode=sht.Mode.SPLIT)
+    mx, fro = sht.compare(C2, C1)
+    assert 0.0 <= fro <= REL_TOL and mx >= 0.0
