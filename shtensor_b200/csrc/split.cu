@@ -174,9 +174,10 @@ __device__ __forceinline__ void cp16(void* smem, const void* gmem, int bytes) {
                : "memory");
 }
 
-// int32 -> double with one integer move and one add: 2^52 + 2^51 + x has x in its low word
+// int32 -> double with one integer add and one FP64 add: the bits of 1.5*2^52 plus the
+// sign-extended x are the double 1.5*2^52 + x (unit spacing in that binade)
 __device__ __forceinline__ double i2d(unsigned x) {
-  return __hiloint2double(0x43380000, (int)x) - 6755399441055744.0;
+  return __longlong_as_double(0x4338000000000000LL + (long long)(int)x) - 6755399441055744.0;
 }
 
 // ------------------------------------------------------------------ main kernel
