@@ -107,6 +107,23 @@ def dist_env():
     return rank, world, local
 
 
+def reduce_max(x: float) -> float:
+    """Max of x over the ranks of the default process group (1 rank: x itself)."""
+    import torch
+    import torch.distributed as dist
+    if not dist.is_available() or not dist.is_initialized() or dist.get_world_size() == 1:
+        return x
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([x], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def replica_rate(work_per_rank: float, ms_per_rank: float, world: int) -> float:
+    """Whole-job rate of `world` independent replicas timed by their slowest rank (work/ms → work/s/1e6)."""
+    return world * work_per_rank / reduce_max(ms_per_rank) / 1e6
+
+
 def build_workload(args):
     from shtensor_b200 import workloads as W
     return W.c1(seed=args.seed, scale=args.scale)
@@ -237,12 +254,7 @@ def run_ours(args):
         if world > 1:
             torch.distributed.barrier()
 
-    def max_over_ranks(x: float) -> float:
-        if world == 1:
-            return x
-        t = torch.tensor([x], device="cuda", dtype=torch.float64)
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        return float(t.item())
+    max_over_ranks = reduce_max
 
     forms = {"plain": sht.Mode.PLAIN_FP64, "batched": sht.Mode.BATCHED_FP64, "split": sht.Mode.SPLIT}
     results = {}
