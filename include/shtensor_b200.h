@@ -104,6 +104,18 @@ sht_status sht_kernel_create(sht_ctx* ctx, const char* expr, const int* sizes_a,
  * the result is back in host memory. */
 sht_status sht_kernel_call(sht_kernel* k, const void* a, const void* b, void* c, int64_t nb_ops,
                            void* stream);
+/* Allocation-free Kernel<double>::call (no counterpart in the reference).  For callers that
+ * cannot call cudaMalloc -- code inside someone else's CUDA-graph capture, plugin hosts that
+ * only hand over pre-registered buffers, processes whose device memory another runtime has
+ * reserved.  a, b, c are device pointers (the caller passes inputs and outputs); the result
+ * bits equal sht_kernel_call's.  Its only scratch is a static 32 MiB device array that every
+ * GPU loading the library keeps until exit: a stack needing more (nb_ops * (m_pad + n_pad) *
+ * K4 * 8 bytes, m_pad/n_pad rounded up to even, K4 to a multiple of 4) is rejected with
+ * SHT_ERR_SIZE.  The first call on a device looks the array up (cudaGetSymbolAddress) and
+ * should come before any stream capture.  Calls share the array: calls that overlap on the
+ * GPU race. */
+sht_status sht_kernel_call_static(sht_kernel* k, const double* a, const double* b, double* c, int64_t nb_ops,
+                                  void* stream);
 sht_status sht_kernel_info(sht_kernel* k, char* buf, size_t len);
 sht_status sht_kernel_destroy(sht_kernel* k);
 

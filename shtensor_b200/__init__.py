@@ -83,6 +83,7 @@ _SIGS = {
     "sht_kernel_create": [_P, C.c_char_p, _P, C.c_int, _P, C.c_int, _P, C.c_int, C.c_double, C.c_double, C.c_int,
                           C.c_int, C.POINTER(_P)],
     "sht_kernel_call": [_P, _P, _P, _P, C.c_int64, _P],
+    "sht_kernel_call_static": [_P, _P, _P, _P, C.c_int64, _P],
     "sht_kernel_info": [_P, C.c_char_p, C.c_size_t],
     "sht_kernel_destroy": [_P],
     "sht_tensor_create": [_P, C.c_int, _P, _P, C.c_int, C.POINTER(_P)],
@@ -239,6 +240,14 @@ class Kernel:
         """a, b, c: torch CUDA tensors (run on `stream`) or numpy arrays (staged, synchronous)."""
         _check(lib().sht_kernel_call(self._h, _P(_ptr(a)), _P(_ptr(b)), _P(_ptr(c)), C.c_int64(nb_ops),
                                      _stream(stream)))
+        return c
+
+    def call_static(self, a, b, c, nb_ops: int, stream=None):
+        """Allocation-free call for callers that cannot allocate device memory: a, b, c are
+        device buffers (torch CUDA tensors or raw pointers); scratch is a static device array
+        of 32 MiB shared by all such calls, so calls that overlap on the GPU race."""
+        _check(lib().sht_kernel_call_static(self._h, _P(_ptr(a)), _P(_ptr(b)), _P(_ptr(c)), C.c_int64(nb_ops),
+                                            _stream(stream)))
         return c
 
     def get_info(self) -> str:

@@ -9,6 +9,7 @@
 namespace sht {
 
 double measure_fp64_tflops(sht_ctx* ctx);
+void stack_call_static(sht_kernel* k, const double* a, const double* b, double* c, int64_t nb_ops, cudaStream_t s);
 
 static void prepare_mode(sht_plan* p, cudaStream_t s) {
   if (p->mode == SHT_MODE_BATCHED_FP64) batched_prepare(p, s);
@@ -161,6 +162,14 @@ sht_status sht_kernel_call(sht_kernel* k, const void* a, const void* b, void* c,
   return guard([&] {
     need(k, "null kernel");
     stack_call(k, a, b, c, nb_ops, as_stream(stream));
+  });
+}
+
+sht_status sht_kernel_call_static(sht_kernel* k, const double* a, const double* b, double* c, int64_t nb_ops,
+                                  void* stream) {
+  return guard([&] {
+    need(k, "null kernel");
+    stack_call_static(k, a, b, c, nb_ops, as_stream(stream));
   });
 }
 
