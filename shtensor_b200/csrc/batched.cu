@@ -212,8 +212,11 @@ static void launch_batched(sht_plan* p, BatchedArgs& b, cudaStream_t s) {
 void batched_prepare(sht_plan* p, cudaStream_t s) {
   p->d_counter = PoolBuf(p->ctx->pool.get(), 256, s);
   matform_prepare(p, s);
+  trace("batched: matform layout", s);
   const HostPlanView v = host_view(p, s);
+  trace("batched: host view", s);
   build_batched_work(p, v, p->ctx->tuned, s);
+  trace("batched: work list", s);
 }
 
 
@@ -238,7 +241,9 @@ void batched_execute(sht_plan* p, const SparseArgs& g, long long, cudaStream_t s
   b.nwork = (int)((bb == one) ? p->bwork_touched : p->bwork);
   b.counter = p->d_counter.as<int>();
   if (!g.sc.alpha_zero) matform_execute(p, g.sc.alpha, s);
+  trace("batched: matform kernels", s);
   launch_batched(p, b, s);
+  trace("batched: tile kernel", s);
 }
 
 // ------------------------------------------------------------------ autotuner

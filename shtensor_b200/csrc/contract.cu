@@ -17,6 +17,7 @@
 
 #include <algorithm>
 #include <chrono>
+#include <cstdlib>
 #include <cstring>
 
 #include "contract.h"
@@ -27,6 +28,19 @@ namespace sht {
 
 double now_ms() {
   return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now().time_since_epoch()).count();
+}
+
+void trace(const char* what, cudaStream_t s) {
+  static const bool on = [] {
+    const char* e = std::getenv("SHT_TRACE");
+    return e && e[0] == '1';
+  }();
+  if (!on) return;
+  static double last = 0;
+  cudaStreamSynchronize(s);
+  const double t = now_ms();
+  std::fprintf(stderr, "[sht] %-28s %8.3f ms\n", what, last > 0 ? t - last : 0.0);
+  last = t;
 }
 
 // ---------------------------------------------------------------------------------------
@@ -290,6 +304,7 @@ static int choose_plain_shape(const sht_plan* p) {
 sht_plan* plan_create(sht_ctx* ctx, const std::string& expr, sht_tensor* A, sht_tensor* B, sht_tensor* C,
                       double eps, sht_norm norm, sht_mode mode, cudaStream_t s) {
   const double t0 = now_ms();
+  trace("plan: start", s);
   if (!A || !B || !C) fail(SHT_ERR_INVALID, "null tensor");
   if (A->ctx != ctx || B->ctx != ctx || C->ctx != ctx) fail(SHT_ERR_INVALID, "tensors from another context");
   if (A->dtype != SHT_F64 || B->dtype != SHT_F64 || C->dtype != SHT_F64)
@@ -399,6 +414,7 @@ sht_plan* plan_create(sht_ctx* ctx, const std::string& expr, sht_tensor* A, sht_
     }
   }
   p->npairs = np;
+  trace("plan: match+sort pairs", s);
 
   // result pattern: unique idC ∪ stored C ids
   long long nu = 0;
@@ -476,6 +492,7 @@ sht_plan* plan_create(sht_ctx* ctx, const std::string& expr, sht_tensor* A, sht_
   }
   const long long nc = C->nblocks;
   p->ncblk = nc;
+  trace("plan: result pattern", s);
 
   // pair ranges and work list
   p->d_pstart = PoolBuf(pool, (nc + 1) * 4, s);
@@ -500,6 +517,7 @@ sht_plan* plan_create(sht_ctx* ctx, const std::string& expr, sht_tensor* A, sht_
     }
     p->flops = fl;
   }
+  trace("plan: pstart+flops", s);
   p->tmaps.row = make_modemap(mp.rowA, mp.rowC);
   p->tmaps.kk = make_modemap(mp.colA, mp.rowB);
   p->tmaps.col = make_modemap(mp.colB, mp.colC);
@@ -508,6 +526,7 @@ sht_plan* plan_create(sht_ctx* ctx, const std::string& expr, sht_tensor* A, sht_
   p->tmaps.oC = C->order;
   p->shape = choose_plain_shape(p.get());
   build_work(p.get(), kShapes[p->shape].tm, kShapes[p->shape].tn, s);
+  trace("plan: plain work list", s);
   p->plan_ms = now_ms() - t0;
   return p.release();
 }

@@ -186,5 +186,8 @@ void stack_call(sht_kernel* k, const void* a, const void* b, void* c, int64_t nb
 
 // timing helpers
 double now_ms();
+// Phase trace of the host runtime, printed to stderr when SHT_TRACE=1 (the stream is
+// synchronized at each point so the times are device-inclusive).
+void trace(const char* what, cudaStream_t s);
 
 }  // namespace sht
