@@ -12,7 +12,10 @@
 #include <cstring>
 #include <fstream>
 #include <numeric>
+#include <cstdio>
 #include <sstream>
+
+#include <cub/cub.cuh>
 
 #include "contract.h"
 #include "device_common.cuh"
@@ -209,13 +212,137 @@ static void launch_batched(sht_plan* p, BatchedArgs& b, cudaStream_t s) {
   SHT_CUDA(cudaGetLastError());
 }
 
+// ------------------------------------------------------------------ device work list
+struct ShapeSet {
+  int n;
+  int tm[kNumB], tn[kNumB];
+};
+
+__device__ __forceinline__ int ilog2ceil_dev(long long v) {
+  int b = 0;
+  while ((1LL << b) < v) ++b;
+  return b;
+}
+
+__global__ void k_block_shapes(const int* __restrict__ cm, const int* __restrict__ cn,
+                               const long long* __restrict__ cksum, const int* __restrict__ pstart, long long nc,
+                               const unsigned char* __restrict__ table, int fixed_tm, int fixed_tn, ShapeSet ss,
+                               int* __restrict__ shape, long long* __restrict__ tiles,
+                               long long* __restrict__ touched_tiles, unsigned long long* __restrict__ key,
+                               int* __restrict__ idx) {
+  for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < nc; c += (long long)gridDim.x * blockDim.x) {
+    const long long m = cm[c], n = cn[c], ks = cksum[c];
+    const int np = pstart[c + 1] - pstart[c];
+    int sh = 0;
+    long long tm = fixed_tm, tn = fixed_tn;
+    if (fixed_tm <= 0) {
+      int t = 255;
+      if (table) {
+        const int lm = min(ilog2ceil_dev(m), 31), ln = min(ilog2ceil_dev(n), 31);
+        const int lk = min(ilog2ceil_dev(np > 0 ? (ks / np > 0 ? ks / np : 1) : 1), 31);
+        t = table[(lm * 32 + ln) * 32 + lk];
+      }
+      if (t != 255) {
+        sh = t;
+      } else {  // padded-area model, as on the host
+        double best = 1e300;
+        for (int q = 0; q < ss.n; ++q) {
+          const long long a = ss.tm[q], b = ss.tn[q];
+          const long long nt = ((m + a - 1) / a) * ((n + b - 1) / b);
+          const double cost = (double)nt * (double)(a * b) + 3072.0 * (double)nt;
+          if (cost < best) { best = cost; sh = q; }
+        }
+      }
+      tm = ss.tm[sh];
+      tn = ss.tn[sh];
+    }
+    const long long nt = ((m + tm - 1) / tm) * ((n + tn - 1) / tn);
+    shape[c] = sh;
+    tiles[c] = nt;
+    touched_tiles[c] = np > 0 ? nt : 0;
+    key[c] = np > 0 ? (unsigned long long)(tm * tn) * (unsigned long long)ks + 1ull : 0ull;
+    idx[c] = (int)c;
+  }
+}
+
+__global__ void k_gather_tiles(const int* __restrict__ idx, const long long* __restrict__ tiles, long long nc,
+                               long long* __restrict__ out) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < nc; i += (long long)gridDim.x * blockDim.x)
+    out[i] = tiles[idx[i]];
+}
+
+__global__ void k_emit_items(const int* __restrict__ idx, const long long* __restrict__ tiles_sorted,
+                             const long long* __restrict__ off, const int* __restrict__ shape, long long nc,
+                             int4* __restrict__ work) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < nc; i += (long long)gridDim.x * blockDim.x) {
+    const int c = idx[i];
+    const long long w0 = off[i];
+    for (long long t = 0; t < tiles_sorted[i]; ++t) work[w0 + t] = make_int4(c, (int)t, shape[c], 0);
+  }
+}
+
+void device_work_list(sht_plan* p, int fixed_tm, int fixed_tn, bool per_class, cudaStream_t s) {
+  DevicePool* pool = p->ctx->pool.get();
+  const long long nc = p->ncblk;
+  p->bwork = p->bwork_touched = 0;
+  if (nc == 0) {
+    p->d_bwork = PoolBuf(pool, sizeof(int4), s);
+    return;
+  }
+  ShapeSet ss{};
+  ss.n = kNumB;
+  for (int q = 0; q < kNumB; ++q) { ss.tm[q] = kBTM[q]; ss.tn[q] = kBTN[q]; }
+  PoolBuf table;
+  if (per_class && !p->ctx->tuned.empty()) {
+    std::vector<unsigned char> h(32 * 32 * 32, 255);
+    for (auto& kv : p->ctx->tuned) {
+      int lm, ln, lk;
+      if (std::sscanf(kv.first.c_str(), "%d,%d,%d", &lm, &ln, &lk) == 3 && lm < 32 && ln < 32 && lk < 32)
+        h[(lm * 32 + ln) * 32 + lk] = (unsigned char)kv.second;
+    }
+    table = PoolBuf(pool, h.size(), s);
+    SHT_CUDA(cudaMemcpyAsync(table.ptr, h.data(), h.size(), cudaMemcpyHostToDevice, s));
+    SHT_CUDA(cudaStreamSynchronize(s));  // pageable source
+  }
+  PoolBuf shape(pool, nc * 4, s), tiles(pool, nc * 8, s), ttiles(pool, nc * 8, s), key(pool, nc * 8, s),
+      idx(pool, nc * 4, s), key2(pool, nc * 8, s), idx2(pool, nc * 4, s), tsorted(pool, nc * 8, s),
+      off(pool, nc * 8, s), sums(pool, 16, s);
+  k_block_shapes<<<grid_for(nc, 256), 256, 0, s>>>(
+      p->d_cm.as<int>(), p->d_cn.as<int>(), p->d_cksum.as<long long>(), p->d_pstart.as<int>(), nc,
+      table.as<unsigned char>(), per_class ? 0 : fixed_tm, fixed_tn, ss, shape.as<int>(), tiles.as<long long>(),
+      ttiles.as<long long>(), key.as<unsigned long long>(), idx.as<int>());
+  SHT_CUDA(cudaGetLastError());
+  size_t tb = 0, tb2 = 0, tb3 = 0;
+  cub::DeviceRadixSort::SortPairsDescending(nullptr, tb, key.as<unsigned long long>(), key2.as<unsigned long long>(),
+                                            idx.as<int>(), idx2.as<int>(), (int)nc, 0, 64, s);
+  cub::DeviceScan::ExclusiveSum(nullptr, tb2, tsorted.as<long long>(), off.as<long long>(), (int)nc, s);
+  cub::DeviceReduce::Sum(nullptr, tb3, ttiles.as<long long>(), sums.as<long long>(), (int)nc, s);
+  PoolBuf tmp(pool, std::max(tb, std::max(tb2, tb3)), s);
+  cub::DeviceRadixSort::SortPairsDescending(tmp.ptr, tb, key.as<unsigned long long>(), key2.as<unsigned long long>(),
+                                            idx.as<int>(), idx2.as<int>(), (int)nc, 0, 64, s);
+  k_gather_tiles<<<grid_for(nc, 256), 256, 0, s>>>(idx2.as<int>(), tiles.as<long long>(), nc, tsorted.as<long long>());
+  cub::DeviceScan::ExclusiveSum(tmp.ptr, tb2, tsorted.as<long long>(), off.as<long long>(), (int)nc, s);
+  cub::DeviceReduce::Sum(tmp.ptr, tb3, ttiles.as<long long>(), sums.as<long long>(), (int)nc, s);
+  long long h[3];
+  SHT_CUDA(cudaMemcpyAsync(&h[0], off.as<long long>() + nc - 1, 8, cudaMemcpyDeviceToHost, s));
+  SHT_CUDA(cudaMemcpyAsync(&h[1], tsorted.as<long long>() + nc - 1, 8, cudaMemcpyDeviceToHost, s));
+  SHT_CUDA(cudaMemcpyAsync(&h[2], sums.ptr, 8, cudaMemcpyDeviceToHost, s));
+  SHT_CUDA(cudaStreamSynchronize(s));
+  const long long total = h[0] + h[1];
+  if (total > (long long)INT32_MAX) fail(SHT_ERR_UNSUPPORTED, "work list above 2^31 tiles");
+  p->bwork = total;
+  p->bwork_touched = h[2];
+  p->d_bwork = PoolBuf(pool, std::max(total, 1LL) * sizeof(int4), s);
+  k_emit_items<<<grid_for(nc, 128), 128, 0, s>>>(idx2.as<int>(), tsorted.as<long long>(), off.as<long long>(),
+                                                  shape.as<int>(), nc, p->d_bwork.as<int4>());
+  SHT_CUDA(cudaGetLastError());
+}
+
 void batched_prepare(sht_plan* p, cudaStream_t s) {
   p->d_counter = PoolBuf(p->ctx->pool.get(), 256, s);
   matform_prepare(p, s);
   trace("batched: matform layout", s);
-  const HostPlanView v = host_view(p, s);
-  trace("batched: host view", s);
-  build_batched_work(p, v, p->ctx->tuned, s);
+  device_work_list(p, 0, 0, true, s);
   trace("batched: work list", s);
 }
 
@@ -327,7 +454,7 @@ void autotune(sht_plan* p, const char* cache_file, cudaStream_t s) {
     std::ofstream out(cache_file, std::ios::app);
     for (auto& kv : ctx->tuned) out << gpu << " " << kv.first << " " << kv.second << "\n";
   }
-  build_batched_work(p, v, ctx->tuned, s);
+  device_work_list(p, 0, 0, true, s);
 }
 
 }  // namespace sht

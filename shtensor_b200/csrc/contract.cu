@@ -301,6 +301,49 @@ static int choose_plain_shape(const sht_plan* p) {
   return best_i;
 }
 
+// per C block: matrix extents m, n, the sum over its pairs of the contracted extent, flops
+__global__ void k_cstats(const int* __restrict__ dimsC, int oC, ModeMap row, ModeMap col,
+                         const int* __restrict__ pstart, const int* __restrict__ pair_a,
+                         const int* __restrict__ dimsA, int oA, ModeMap kk, long long nc, int* __restrict__ m_out,
+                         int* __restrict__ n_out, long long* __restrict__ ksum_out, double* __restrict__ flops_out) {
+  for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < nc; c += (long long)gridDim.x * blockDim.x) {
+    long long m = 1, n = 1, ks = 0;
+    for (int t = 0; t < row.n; ++t) m *= dimsC[c * oC + row.y[t]];
+    for (int t = 0; t < col.n; ++t) n *= dimsC[c * oC + col.y[t]];
+    for (int p = pstart[c]; p < pstart[c + 1]; ++p) {
+      const int* ad = dimsA + (long long)pair_a[p] * oA;
+      long long k = 1;
+      for (int t = 0; t < kk.n; ++t) k *= ad[kk.x[t]];
+      ks += k;
+    }
+    m_out[c] = (int)m;
+    n_out[c] = (int)n;
+    ksum_out[c] = ks;
+    flops_out[c] = 2.0 * (double)m * (double)n * (double)ks;
+  }
+}
+
+void cblock_stats(sht_plan* p, cudaStream_t s) {
+  DevicePool* pool = p->ctx->pool.get();
+  const long long nc = p->ncblk;
+  p->d_cm = PoolBuf(pool, std::max(nc, 1LL) * 4, s);
+  p->d_cn = PoolBuf(pool, std::max(nc, 1LL) * 4, s);
+  p->d_cksum = PoolBuf(pool, std::max(nc, 1LL) * 8, s);
+  p->flops = 0.0;
+  if (nc == 0) return;
+  PoolBuf fl(pool, nc * 8, s), tot(pool, 8, s);
+  k_cstats<<<grid_for(nc, 256), 256, 0, s>>>(p->C->d_dims.as<int>(), p->C->order, p->tmaps.row, p->tmaps.col,
+                                              p->d_pstart.as<int>(), p->d_pair_a.as<int>(), p->A->d_dims.as<int>(),
+                                              p->A->order, p->tmaps.kk, nc, p->d_cm.as<int>(), p->d_cn.as<int>(),
+                                              p->d_cksum.as<long long>(), fl.as<double>());
+  SHT_CUDA(cudaGetLastError());
+  size_t tb = 0;
+  cub::DeviceReduce::Sum(nullptr, tb, fl.as<double>(), tot.as<double>(), (int)nc, s);
+  PoolBuf tmp(pool, tb, s);
+  cub::DeviceReduce::Sum(tmp.ptr, tb, fl.as<double>(), tot.as<double>(), (int)nc, s);
+  p->flops = d2h_scalar<double>(tot.ptr, s);
+}
+
 sht_plan* plan_create(sht_ctx* ctx, const std::string& expr, sht_tensor* A, sht_tensor* B, sht_tensor* C,
                       double eps, sht_norm norm, sht_mode mode, cudaStream_t s) {
   const double t0 = now_ms();
@@ -500,33 +543,20 @@ sht_plan* plan_create(sht_ctx* ctx, const std::string& expr, sht_tensor* A, sht_
                                                   p->d_pstart.as<int>());
   SHT_CUDA(cudaGetLastError());
   p->flops = 0;
-  // flop count on the host from the pair list (block extents are on the host)
-  if (np > 0) {
-    std::vector<int> ha(np), hb(np);
-    SHT_CUDA(cudaMemcpyAsync(ha.data(), p->d_pair_a.ptr, np * 4, cudaMemcpyDeviceToHost, s));
-    SHT_CUDA(cudaMemcpyAsync(hb.data(), p->d_pair_b.ptr, np * 4, cudaMemcpyDeviceToHost, s));
-    SHT_CUDA(cudaStreamSynchronize(s));
-    double fl = 0;
-    for (long long i = 0; i < np; ++i) {
-      const int64_t ida = A->ids[ha[i]], idb = B->ids[hb[i]];
-      double m = 1, n = 1, k = 1;
-      for (int ax : mp.rowA) m *= A->bs[ax][(ida / A->gstride[ax]) % A->nblk[ax]];
-      for (int ax : mp.colA) k *= A->bs[ax][(ida / A->gstride[ax]) % A->nblk[ax]];
-      for (int ax : mp.colB) n *= B->bs[ax][(idb / B->gstride[ax]) % B->nblk[ax]];
-      fl += 2.0 * m * n * k;
-    }
-    p->flops = fl;
-  }
-  trace("plan: pstart+flops", s);
   p->tmaps.row = make_modemap(mp.rowA, mp.rowC);
   p->tmaps.kk = make_modemap(mp.colA, mp.rowB);
   p->tmaps.col = make_modemap(mp.colB, mp.colC);
   p->tmaps.oA = A->order;
   p->tmaps.oB = B->order;
   p->tmaps.oC = C->order;
-  p->shape = choose_plain_shape(p.get());
-  build_work(p.get(), kShapes[p->shape].tm, kShapes[p->shape].tn, s);
-  trace("plan: plain work list", s);
+  // per C block m, n, sum of the pairs' k and flops; the total flop count
+  cblock_stats(p.get(), s);
+  trace("plan: pstart+flops", s);
+  if (mode == SHT_MODE_PLAIN_FP64) {
+    p->shape = choose_plain_shape(p.get());
+    build_work(p.get(), kShapes[p->shape].tm, kShapes[p->shape].tn, s);
+    trace("plan: plain work list", s);
+  }
   p->plan_ms = now_ms() - t0;
   return p.release();
 }

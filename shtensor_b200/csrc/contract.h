@@ -17,6 +17,7 @@ struct sht_plan {
   sht::PoolBuf d_pair_a, d_pair_b;  // int32 storage indices into A / B, canonical order
   sht::PoolBuf d_pstart;            // int32[ncblk + 1]
   sht::PoolBuf d_work;              // int2 (C block, tile) for the plain path
+  sht::PoolBuf d_cm, d_cn, d_cksum; // per C block: rows, columns, sum of the pairs' k
   // batched path
   sht::PoolBuf d_bwork;             // int4 (C block, tile, class, 0)
   sht::PoolBuf d_counter;           // work counter of the persistent kernel
@@ -47,6 +48,10 @@ namespace sht {
 sht_plan* plan_create(sht_ctx* ctx, const std::string& expr, sht_tensor* A, sht_tensor* B, sht_tensor* C,
                       double eps, sht_norm norm, sht_mode mode, cudaStream_t s);
 void build_work(sht_plan* p, int TM, int TN, cudaStream_t s);
+void cblock_stats(sht_plan* p, cudaStream_t s);
+// Cost-ordered work list (C block, tile, shape) on the device: fixed_shape >= 0 uses one
+// shape (tm x tn) for every block, otherwise per size class from class_shape (or the model).
+void device_work_list(sht_plan* p, int fixed_tm, int fixed_tn, bool per_class, cudaStream_t s);
 void plan_execute(sht_plan* p, double alpha, double beta, cudaStream_t s);
 void batched_prepare(sht_plan* p, cudaStream_t s);
 void batched_execute(sht_plan* p, const SparseArgs& g, long long nwork_plain, cudaStream_t s);

@@ -190,7 +190,7 @@ struct SplitArgs {
   const int* dimsA; const int* dimsB;
   double* C; const long long* offC; const int* dimsC;
   const int* pair_a; const int* pair_b; const int* pstart;
-  const int2* work;
+  const int4* work;
   int nwork;
   int* counter;
   int* err;
@@ -241,7 +241,7 @@ __global__ void __launch_bounds__(128, 1) k_split(SplitArgs g) {
     const int item = sm.item;
     __syncthreads();
     if (item >= g.nwork || failed) break;
-    const int2 w = g.work[item];
+    const int4 w = g.work[item];
     const int c = w.x;
     double* cptr = g.C + g.offC[c];
     const int* cd = g.dimsC + (long long)c * g.mp.oC;
@@ -448,26 +448,8 @@ void split_prepare(sht_plan* p, int S, cudaStream_t s) {
   }
   SHT_CUDA(cudaMemsetAsync(p->sp_err.ptr, 0, 256, s));
   SHT_CUDA(cudaStreamSynchronize(s));
-  // work list: 128 x 32 tiles of every C block
-  tensor_sync_host(p->C, s);
-  std::vector<int> ps(p->ncblk + 1);
-  SHT_CUDA(cudaMemcpyAsync(ps.data(), p->d_pstart.ptr, (p->ncblk + 1) * 4, cudaMemcpyDeviceToHost, s));
-  SHT_CUDA(cudaStreamSynchronize(s));
-  std::vector<int2> touched, untouched;
-  for (long long c = 0; c < p->ncblk; ++c) {
-    const int64_t id = p->C->ids[c];
-    long long m = 1, n = 1;
-    for (int ax : p->maps.rowC) m *= p->C->bs[ax][(id / p->C->gstride[ax]) % p->C->nblk[ax]];
-    for (int ax : p->maps.colC) n *= p->C->bs[ax][(id / p->C->gstride[ax]) % p->C->nblk[ax]];
-    const long long tiles = ((m + kSplitM - 1) / kSplitM) * ((n + kSplitN - 1) / kSplitN);
-    for (long long t = 0; t < tiles; ++t) (ps[c + 1] > ps[c] ? touched : untouched).push_back(make_int2((int)c, (int)t));
-  }
-  p->bwork_touched = (long long)touched.size();
-  touched.insert(touched.end(), untouched.begin(), untouched.end());
-  p->bwork = (long long)touched.size();
-  p->d_bwork = PoolBuf(pool, std::max<size_t>(touched.size(), 1) * sizeof(int2), s);
-  if (!touched.empty())
-    SHT_CUDA(cudaMemcpyAsync(p->d_bwork.ptr, touched.data(), touched.size() * sizeof(int2), cudaMemcpyHostToDevice, s));
+  // work list: 128 x 32 tiles of every C block, heaviest blocks first
+  device_work_list(p, kSplitM, kSplitN, false, s);
   p->d_counter = PoolBuf(pool, 256, s);
   SHT_CUDA(cudaStreamSynchronize(s));
 }
@@ -521,7 +503,7 @@ void split_execute(sht_plan* p, const SparseArgs& sa, cudaStream_t s) {
   g.dimsA = p->A->d_dims.as<int>(); g.dimsB = p->B->d_dims.as<int>();
   g.C = sa.C; g.offC = sa.offC; g.dimsC = sa.dimsC;
   g.pair_a = sa.pair_a; g.pair_b = sa.pair_b; g.pstart = sa.pstart;
-  g.work = p->d_bwork.as<int2>();
+  g.work = p->d_bwork.as<int4>();
   g.nwork = (int)((bb == one) ? p->bwork_touched : p->bwork);
   g.counter = p->d_counter.as<int>();
   g.err = p->sp_err.as<int>();
