@@ -321,9 +321,17 @@ def run_ours(args):
         lambda: sht.contract(ctx, w.expr, 1.0, A, B, 0.0, Cd, mode=forms[best], stream=stream))
     peak = measure_fp64_peak(sht, ctx)
     achieved = prep["flops"] / kern_ms / 1e9  # TFLOP/s
+    traffic = None
+    try:  # DRAM bytes per launch of the dominant kernel, from the committed ncu summary
+        with open(os.path.join(ROOT, "profiles", "roofline_traffic.json")) as f:
+            traffic = json.load(f).get(best, {}).get("traffic_bytes_per_launch")
+    except (OSError, ValueError):
+        traffic = None
     roofline = {"bound": "tensor", "pipe": "fp64 (DFMA; B200's FP64 and FP64-tensor peaks are the same figure)",
                 "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
-                "frac": (achieved / peak) if peak else None, "traffic": None,
+                "frac": (achieved / peak) if peak else None, "traffic": traffic,
+                "traffic_source": "profiles/roofline_traffic.json (ncu capture at scale 0.5, scaled by C elements)",
+                "algorithmic_bytes": 8.0 * (Cd.nnz + w.A.nnz + w.B.nnz),
                 "peak_source": "measured in this run by the library's FP64 FMA-chain kernel" if peak else "unmeasured",
                 "kernel_ms": kern_ms,
                 "kernel": {"plain": "k_contract_tiles", "batched": "k_matform + k_batched",
