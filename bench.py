@@ -52,6 +52,11 @@ def parse():
     ap.add_argument("--no-count", action="store_true", help="skip the CUPTI launch count (use under ncu)")
     ap.add_argument("--no-autotune", action="store_true")
     ap.add_argument("--pool-gb", type=float, default=60.0)
+    ap.add_argument("--no-serving", action="store_true", help="skip the serving-loop phase")
+    ap.add_argument("--serve-rate", type=float, default=200.0, help="Poisson arrival rate (requests/s)")
+    ap.add_argument("--serve-seconds", type=float, default=2.0, help="length of the arrival stream")
+    ap.add_argument("--serve-templates", type=int, default=16,
+                    help="distinct requests (resident inputs) the stream draws from")
     return ap.parse_args()
 
 
@@ -197,6 +202,110 @@ def measure_fp64_peak(sht, ctx):
         return None
 
 
+def run_serving(args, sht, ctx, upload, server_kwargs=None):
+    """Serving phase: a seeded Poisson stream of mixed contractions through sht.Server.
+
+    Requests are drawn from `serve_templates` distinct contractions of the c0..c3 families
+    (extents x U(0.25,1), occupancy U(0.05,0.4)), whose inputs stay resident; each request
+    writes its own fresh C, released when it completes.  Reported beside it: the same
+    requests each run alone on the plain FP64 path (synchronous sht_contract, no queueing),
+    a burst of the whole stream submitted at once (the loop's capacity), and a bit-equality
+    check of served results against the same requests run alone."""
+    from shtensor_b200 import workloads as W
+    rng = np.random.default_rng(args.seed + 1000)
+    t_gen = time.perf_counter()
+    temps = [W.c4_request(rng) for _ in range(args.serve_templates)]
+    gen_s = time.perf_counter() - t_gen
+    ins = [(upload(w.A), upload(w.B)) for w in temps]
+    n = max(1, int(round(args.serve_rate * args.serve_seconds)))
+    picks = rng.integers(0, len(temps), n)
+    arrivals = np.cumsum(rng.exponential(1.0 / args.serve_rate, n))
+
+    def fresh_c(w):
+        return upload(W.empty_tensor(w.C.block_sizes))
+
+    # each template alone on the plain path: plan + execute to completion, median of 3 after one
+    import torch
+    alone_ms, tflops = [], []
+    for w, (A, B) in zip(temps, ins):
+        ts = []
+        for r in range(4):
+            C = fresh_c(w)
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            rep = sht.contract(ctx, w.expr, 1.0, A, B, 0.0, C, w.screen_eps, mode=sht.Mode.PLAIN_FP64)
+            torch.cuda.synchronize()
+            ts.append((time.perf_counter() - t0) * 1e3)
+            del C
+        alone_ms.append(float(np.median(ts[1:])))
+        tflops.append(rep["flops"])
+    alone_stream = np.array([alone_ms[k] for k in picks])
+    stream_flops = float(sum(tflops[k] for k in picks))
+
+    def pct(v, q):
+        v = np.sort(np.asarray(v))
+        return float(v[min(len(v) - 1, max(0, int(np.ceil(q * len(v))) - 1))])
+
+    out = {"rate_per_s": args.serve_rate, "requests": n, "stream_s": float(arrivals[-1]),
+           "templates": [{"family": w.meta["family"], "u": round(w.meta["u"], 3),
+                          "occupancy": round(w.meta["occupancy"], 3), "gflop": f / 1e9,
+                          "alone_plain_ms": a} for w, f, a in zip(temps, tflops, alone_ms)],
+           "template_gen_s": gen_s, "offered_gflops": stream_flops / float(arrivals[-1]) / 1e9}
+    out["alone_plain"] = {"p50_ms": pct(alone_stream, 0.5), "p99_ms": pct(alone_stream, 0.99),
+                          "gflops": stream_flops / (alone_stream.sum() / 1e3) / 1e9,
+                          "busy_s": float(alone_stream.sum() / 1e3)}
+    keep_check = {}
+    with sht.Server(ctx, **(server_kwargs or {})) as srv:
+        # warm-up: every template once
+        for w, (A, B) in zip(temps, ins):
+            C = fresh_c(w)
+            srv.wait(srv.submit(w.expr, 1.0, A, B, 0.0, C, w.screen_eps), 300)
+            del C
+        for phase in ("stream", "burst"):
+            srv.reset_stats()
+            pending = {}
+            reps = []
+            t0 = time.perf_counter()
+            i = 0
+            while i < n or pending:
+                now = time.perf_counter() - t0
+                while i < n and (phase == "burst" or arrivals[i] <= now):
+                    k = int(picks[i])
+                    w, (A, B) = temps[k], ins[k]
+                    C = fresh_c(w)
+                    pending[srv.submit(w.expr, 1.0, A, B, 0.0, C, w.screen_eps)] = (C, k)
+                    i += 1
+                for rid in list(pending):
+                    if srv.poll(rid):
+                        reps.append(srv.wait(rid, 300))
+                        C, k = pending.pop(rid)
+                        if phase == "stream" and k not in keep_check and len(keep_check) < 6:
+                            keep_check[k] = C
+                        del C
+                time.sleep(0.0002)
+            st = srv.stats()
+            out[phase] = {"p50_ms": st["p50_ms"], "p99_ms": st["p99_ms"], "max_ms": st["max_ms"],
+                          "gflops": st["gflops"], "span_s": st["span_s"], "completed": st["completed"],
+                          "failed": st["failed"], "launches": st["batches"], "mean_batch": st["mean_batch"],
+                          "max_active": st["max_active_seen"], "deferrals": st["deferrals"],
+                          "mean_queue_ms": float(np.mean([r["queue_ms"] for r in reps])),
+                          "mean_plan_ms": float(np.mean([r["plan_ms"] for r in reps])),
+                          "mean_run_ms": float(np.mean([r["run_ms"] for r in reps]))}
+    # served results against the same requests run alone (batched and plain give the same bits)
+    same = True
+    for k, Cs in keep_check.items():
+        w, (A, B) = temps[k], ins[k]
+        Cr = fresh_c(w)
+        sht.contract(ctx, w.expr, 1.0, A, B, 0.0, Cr, w.screen_eps, mode=sht.Mode.PLAIN_FP64)
+        mx, _ = sht.compare(Cs, Cr)
+        same = same and Cs.nnz == Cr.nnz and mx == 0.0
+        del Cr
+    out["mix_equals_alone"] = {"checked": len(keep_check), "bit_equal_values": bool(same)}
+    keep_check.clear()
+    del ins
+    return out
+
+
 # ------------------------------------------------------------------------------ arms
 def run_reference(args):
     rank, world, _ = dist_env()
@@ -317,6 +426,7 @@ def run_ours(args):
         plan.close()
         del plan
     kern_ms = exec_ms[best]
+    c_nnz = Cd.nnz
     launches, names = (None, []) if args.no_count else count_launches(
         lambda: sht.contract(ctx, w.expr, 1.0, A, B, 0.0, Cd, mode=forms[best], stream=stream))
     peak = measure_fp64_peak(sht, ctx)
@@ -331,7 +441,7 @@ def run_ours(args):
                 "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
                 "frac": (achieved / peak) if peak else None, "traffic": traffic,
                 "traffic_source": "profiles/roofline_traffic.json (ncu capture at scale 0.5, scaled by C elements)",
-                "algorithmic_bytes": 8.0 * (Cd.nnz + w.A.nnz + w.B.nnz),
+                "algorithmic_bytes": 8.0 * (c_nnz + w.A.nnz + w.B.nnz),
                 "peak_source": "measured in this run by the library's FP64 FMA-chain kernel" if peak else "unmeasured",
                 "kernel_ms": kern_ms,
                 "kernel": {"plain": "k_contract_tiles", "batched": "k_matform + k_batched",
@@ -367,6 +477,11 @@ def run_ours(args):
         cpu = {"value": v, "unit": "GFLOP/s", "cores": os.cpu_count(), "kind": kind, "sample": desc,
                "seconds": secs}
 
+    del A, B, Cd
+    serving = None
+    if world == 1 and not args.no_serving:
+        serving = run_serving(args, sht, ctx, T)
+
     if rank == 0:
         r = results[best]
         line = {
@@ -374,15 +489,15 @@ def run_ours(args):
             "warmup": args.warmup, "ms_per_step": r["ms_per_step"], "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
             "config": {"workload": WORKLOAD, "form": best, "scale": args.scale, "seed": args.seed,
-                       "npairs": r["npairs"], "gflop_per_step": flops / 1e9, "c_nnz": Cd.nnz,
+                       "npairs": r["npairs"], "gflop_per_step": flops / 1e9,
                        "l2": "inputs and output larger than L2 (A+B 168 MB, C 5.9 GB); no flush",
+                       "c_nnz": c_nnz,
                        "parallelism": f"replicas x{world}"},
             "forms": results, "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "clocks": clocks,
             "gpu_launches": (launches * args.steps) if launches is not None else None,
-            "gpu_launches_per_step": launches,
+            "gpu_launches_per_step": launches, "serving": serving,
         }
         print(json.dumps(line), flush=True)
-    del A, B, Cd
     ctx.close()
     if world > 1:
         torch.distributed.destroy_process_group()

@@ -169,6 +169,70 @@ sht_status sht_set_split_slices(sht_ctx* ctx, int slices);
 /* which = 0: FP64 FMA peak of this GPU in TFLOP/s (the FP64 kernels' roofline denominator) */
 sht_status sht_measure_peak(sht_ctx* ctx, int which, double* value);
 
+/* ---- serving loop (no reference counterpart: shtensor has no request loop) ----
+ * A server owns one host thread and its own CUDA streams.  Requests are block-sparse
+ * contractions over device-resident tensors, computed in the batched FP64 form (the result
+ * bits equal sht_contract with SHT_MODE_BATCHED_FP64 or SHT_MODE_PLAIN_FP64 run alone).
+ * Continuous batching: a request that arrives while others run is planned at once (by one of
+ * several planner threads) if a slot is free and the pool has room, and joins the next
+ * persistent launch together with every other planned request; up to two launches are
+ * queued, so the next one starts as soon as the running one drains.  Admission: at most max_active requests planned or running, and a
+ * request is planned only if the pool keeps reserve_bytes free after its estimated scratch;
+ * a plan that runs out of pool memory while other requests hold memory is retried after the
+ * next completion (a deferral).  Requests that write a tensor another active or earlier
+ * queued request reads or writes wait for it, so each tensor sees its requests in order.
+ * Threads: while a server runs, the context's owner thread may create, reserve, upload,
+ * download and destroy tensors and submit/poll/wait; it must not destroy a tensor that an
+ * unfinished request names, nor call sht_contract, sht_plan_* or sht_autotune on the
+ * context.  Latencies are host steady-clock times, submit to observed completion. */
+typedef struct sht_server sht_server;
+
+typedef struct {
+  int max_active;        /* requests planned or running at once (0 = 64) */
+  int max_batch;         /* requests fused into one launch (0 = 32) */
+  size_t reserve_bytes;  /* pool bytes that admission leaves free (0 = none) */
+  int planners;          /* planner threads, each with its own stream (0 = 4) */
+  int ctas_per_sm;       /* persistent CTAs per SM of a serving launch (0 = the most that fit
+                            minus one, leaving room for planning kernels) */
+} sht_server_config;
+
+typedef struct {
+  sht_status status;     /* the request's own result */
+  int64_t npairs;        /* block products after screening */
+  double flops;          /* 2*m*n*k summed over the pairs */
+  double queue_ms;       /* submit -> planning starts */
+  double plan_ms;        /* planning (matching, C pattern, work list, matrix-form layout) */
+  double run_ms;         /* launch -> completion observed */
+  double latency_ms;     /* submit -> completion observed */
+  int64_t batch;         /* id of the launch that computed it (-1 if it never ran) */
+  int batch_size;        /* requests in that launch */
+  int deferrals;         /* admissions put off for pool memory */
+} sht_request_report;
+
+typedef struct {
+  int64_t submitted, completed, failed, batches, deferrals;
+  int max_active_seen;   /* most requests planned or running at once */
+  double mean_batch;     /* requests per launch */
+  double p50_ms, p99_ms, max_ms;  /* latency of the completed requests since the last reset */
+  double flops;          /* algorithmic flops of the completed requests */
+  double span_s;         /* first submit -> last completion */
+  double gflops;         /* flops / span_s / 1e9 */
+} sht_server_stats;
+
+sht_status sht_server_create(sht_ctx* ctx, const sht_server_config* cfg, sht_server** out);
+/* queue C = beta*C + alpha*contract(expr, A, B) with screening eps (0 = none) */
+sht_status sht_server_submit(sht_server* srv, const char* expr, double alpha, sht_tensor* A, sht_tensor* B,
+                             double beta, sht_tensor* C, double eps, sht_norm norm, int64_t* request_id);
+/* *state: 0 queued or running, 1 finished (the report is ready) */
+sht_status sht_server_poll(sht_server* srv, int64_t request_id, int* state);
+/* wait up to timeout_s (< 0: no limit); returns the request's status (SHT_ERR_TIMEOUT if it
+ * is still pending) and forgets the request once it has finished */
+sht_status sht_server_wait(sht_server* srv, int64_t request_id, double timeout_s, sht_request_report* rep);
+sht_status sht_server_get_stats(sht_server* srv, sht_server_stats* out);
+sht_status sht_server_reset_stats(sht_server* srv);
+/* finishes every submitted request, then stops the thread and frees the server */
+sht_status sht_server_destroy(sht_server* srv);
+
 #ifdef __cplusplus
 }
 #endif

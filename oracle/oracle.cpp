@@ -273,28 +273,36 @@ void lapack_triple(const double* a, const double* b, double* c, const int* sA, i
 
 // ---------------------------------------------------------------------------------------
 // Block norms, BlockSpan.h:140-164.
-// FROBENIUS here is the canonical deterministic order shared with the device kernels:
-// 32 strided partial sums p[l] = fma(v_e, v_e, p[l]) over e = l, l+32, ... ascending, then
-// p[l] += p[l+off] for off = 16, 8, 4, 2, 1, and sqrt(p[0]).
+// FROBENIUS and MAXABS use the canonical deterministic order shared with the device
+// kernels: chunks of 4096 consecutive elements; in chunk c, 128 lane values
+// p[j] = op(p[j], v_e) over e = c*4096 + j + 128*i ascending (FROBENIUS: fma(v, v, p),
+// MAXABS: max(p, |v|)); then p[j] op= p[j+h] for h = 64, 32, ..., 1; the chunk values are
+// folded in ascending order starting from chunk 0; FROBENIUS ends with sqrt.
 // FROBENIUS_REFCOMPAT reproduces the reference's int accumulator: acc = int(acc + v*v).
 // ---------------------------------------------------------------------------------------
 double block_norm(const double* d, int64_t n, int norm) {
-  if (norm == 1) {
-    double mx = 0.0;
-    for (int64_t i = 0; i < n; ++i) mx = std::max(mx, std::fabs(d[i]));
-    return mx;
-  }
   if (norm == 2) {
     int acc = 0;
     for (int64_t i = 0; i < n; ++i) acc = (int)((double)acc + d[i] * d[i]);
     return std::sqrt((double)acc);
   }
-  double p[32];
-  for (int l = 0; l < 32; ++l) p[l] = 0.0;
-  for (int64_t e = 0; e < n; ++e) p[e & 31] = std::fma(d[e], d[e], p[e & 31]);
-  for (int off = 16; off >= 1; off >>= 1)
-    for (int l = 0; l < off; ++l) p[l] = p[l] + p[l + off];
-  return std::sqrt(p[0]);
+  const bool maxabs = norm == 1;
+  const int64_t chunk = 4096;
+  const int lanes = 128;
+  double total = 0.0;
+  for (int64_t c = 0; c * chunk < n; ++c) {
+    double p[lanes];
+    for (int j = 0; j < lanes; ++j) p[j] = 0.0;
+    const int64_t base = c * chunk, end = std::min(n, base + chunk);
+    for (int64_t e = base; e < end; ++e) {
+      const int j = (int)((e - base) % lanes);
+      p[j] = maxabs ? std::max(p[j], std::fabs(d[e])) : std::fma(d[e], d[e], p[j]);
+    }
+    for (int h = lanes / 2; h >= 1; h >>= 1)
+      for (int j = 0; j < h; ++j) p[j] = maxabs ? std::max(p[j], p[j + h]) : p[j] + p[j + h];
+    total = c == 0 ? p[0] : (maxabs ? std::max(total, p[0]) : total + p[0]);
+  }
+  return maxabs ? total : std::sqrt(total);
 }
 
 // ---------------------------------------------------------------------------------------

@@ -71,6 +71,30 @@ class Report(C.Structure):
         return {k: getattr(self, k) for k, _ in self._fields_ if k != "reserved"}
 
 
+class ServerConfig(C.Structure):
+    _fields_ = [("max_active", C.c_int), ("max_batch", C.c_int), ("reserve_bytes", C.c_size_t),
+                ("planners", C.c_int), ("ctas_per_sm", C.c_int)]
+
+
+class RequestReport(C.Structure):
+    _fields_ = [("status", C.c_int), ("npairs", C.c_int64), ("flops", C.c_double), ("queue_ms", C.c_double),
+                ("plan_ms", C.c_double), ("run_ms", C.c_double), ("latency_ms", C.c_double),
+                ("batch", C.c_int64), ("batch_size", C.c_int), ("deferrals", C.c_int)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+class ServerStats(C.Structure):
+    _fields_ = [("submitted", C.c_int64), ("completed", C.c_int64), ("failed", C.c_int64), ("batches", C.c_int64),
+                ("deferrals", C.c_int64), ("max_active_seen", C.c_int), ("mean_batch", C.c_double),
+                ("p50_ms", C.c_double), ("p99_ms", C.c_double), ("max_ms", C.c_double), ("flops", C.c_double),
+                ("span_s", C.c_double), ("gflops", C.c_double)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
 _P = C.c_void_p
 _SIGS = {
     "sht_init": [C.POINTER(_P), C.c_int, C.c_size_t],
@@ -110,6 +134,14 @@ _SIGS = {
     "sht_autotune": [_P, C.c_char_p, _P],
     "sht_measure_peak": [_P, C.c_int, C.POINTER(C.c_double)],
     "sht_set_split_slices": [_P, C.c_int],
+    "sht_server_create": [_P, C.POINTER(ServerConfig), C.POINTER(_P)],
+    "sht_server_submit": [_P, C.c_char_p, C.c_double, _P, _P, C.c_double, _P, C.c_double, C.c_int,
+                          C.POINTER(C.c_int64)],
+    "sht_server_poll": [_P, C.c_int64, C.POINTER(C.c_int)],
+    "sht_server_wait": [_P, C.c_int64, C.c_double, C.POINTER(RequestReport)],
+    "sht_server_get_stats": [_P, C.POINTER(ServerStats)],
+    "sht_server_reset_stats": [_P],
+    "sht_server_destroy": [_P],
 }
 
 
@@ -413,3 +445,69 @@ def compare(X: Tensor, Ref: Tensor, stream=None):
     mx, fr = C.c_double(), C.c_double()
     _check(lib().sht_tensor_compare(X.handle, Ref.handle, C.byref(mx), C.byref(fr), _stream(stream)))
     return mx.value, fr.value
+
+
+class Server:
+    """Serving loop: continuous batching of contractions over device-resident tensors.
+
+    ``submit`` queues ``C = beta*C + alpha*contract(expr, A, B)`` and returns a request id;
+    ``wait`` returns the request's report (and raises if the request failed).  Results equal
+    :func:`contract` in ``Mode.BATCHED_FP64`` (and ``Mode.PLAIN_FP64``) bit for bit.  The
+    tensors of a request must stay alive and unmodified until it has finished.
+    """
+
+    def __init__(self, ctx: Context, max_active: int = 0, max_batch: int = 0, reserve_bytes: int = 0,
+                 planners: int = 0, ctas_per_sm: int = 0):
+        cfg = ServerConfig(max_active, max_batch, reserve_bytes, planners, ctas_per_sm)
+        h = _P()
+        _check(lib().sht_server_create(ctx.handle, C.byref(cfg), C.byref(h)))
+        self._h = h
+        self.ctx = ctx
+        self._refs = {}
+
+    def submit(self, expr: str, alpha: float, A: Tensor, B: Tensor, beta: float, Cten: Tensor,
+               screen_eps: float = 0.0, norm: BlockNorm = BlockNorm.FROBENIUS) -> int:
+        rid = C.c_int64()
+        _check(lib().sht_server_submit(self._h, expr.encode(), alpha, A.handle, B.handle, beta, Cten.handle,
+                                       screen_eps, int(norm), C.byref(rid)))
+        self._refs[rid.value] = (A, B, Cten)
+        return rid.value
+
+    def poll(self, rid: int) -> bool:
+        st = C.c_int()
+        _check(lib().sht_server_poll(self._h, rid, C.byref(st)))
+        return bool(st.value)
+
+    def wait(self, rid: int, timeout: float = -1.0) -> dict:
+        rep = RequestReport()
+        rc = lib().sht_server_wait(self._h, rid, timeout, C.byref(rep))
+        if rc != Status.ERR_TIMEOUT:
+            self._refs.pop(rid, None)
+        _check(rc)
+        return rep.as_dict()
+
+    def stats(self) -> dict:
+        st = ServerStats()
+        _check(lib().sht_server_get_stats(self._h, C.byref(st)))
+        return st.as_dict()
+
+    def reset_stats(self):
+        _check(lib().sht_server_reset_stats(self._h))
+
+    def close(self):
+        if getattr(self, "_h", None) and _lib is not None:
+            _check(_lib.sht_server_destroy(self._h))
+            self._h = None
+            self._refs.clear()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -46,6 +46,11 @@ struct BatchedArgs {
   const int4* work;
   int nwork;
   int* counter;
+  // serving launch: the requests' descriptors; request r owns launch items
+  // [multi[r].first, multi[r].first + multi[r].nwork)
+  const BatchedArgs* multi;
+  int nmulti;
+  int first;
 };
 
 template <class Cfg>
@@ -67,32 +72,64 @@ __device__ __forceinline__ void run_item(const BatchedArgs& g, int4 w, unsigned 
   tile_run_pipe<Cfg>(g.mp, g.sc, w.y, getc, getpair, g.pstart[c], g.pstart[c + 1], sm);
 }
 
+// Persistent kernel: each CTA takes items off the shared counter until the list is drained.
+// kMulti: the work of several executes in one launch (serving); a launch item is mapped to
+// its request by a binary search over the requests' first items.
+template <bool kMulti>
 __global__ void __launch_bounds__(128, 4) k_batched(BatchedArgs g) {
   extern __shared__ __align__(16) unsigned char smem[];
-  __shared__ int s_item;
+  __shared__ int s_item, s_req;
   for (;;) {
-    if (threadIdx.x == 0) s_item = atomicAdd(g.counter, 1);
+    if (threadIdx.x == 0) {
+      const int item = atomicAdd(g.counter, 1);
+      s_item = item;
+      if (kMulti && item < g.nwork) {
+        int lo = 0, hi = g.nmulti - 1;  // last request whose first item <= item
+        while (lo < hi) {
+          const int mid = (lo + hi + 1) >> 1;
+          if (g.multi[mid].first <= item) lo = mid; else hi = mid - 1;
+        }
+        s_req = lo;
+      }
+    }
     __syncthreads();
     const int item = s_item;
+    const int req = kMulti ? s_req : 0;
     __syncthreads();
     if (item >= g.nwork) break;
-    const int4 w = g.work[item];
-    switch (w.z) {
-      case 0: run_item<B0>(g, w, smem); break;
-      case 1: run_item<B1>(g, w, smem); break;
-      case 2: run_item<B2>(g, w, smem); break;
-      default: run_item<B3>(g, w, smem); break;
+    if constexpr (kMulti) {
+      const BatchedArgs& r = g.multi[req];
+      const int4 w = r.work[item - r.first];
+      switch (w.z) {
+        case 0: run_item<B0>(r, w, smem); break;
+        case 1: run_item<B1>(r, w, smem); break;
+        case 2: run_item<B2>(r, w, smem); break;
+        default: run_item<B3>(r, w, smem); break;
+      }
+    } else {
+      const int4 w = g.work[item];
+      switch (w.z) {
+        case 0: run_item<B0>(g, w, smem); break;
+        case 1: run_item<B1>(g, w, smem); break;
+        case 2: run_item<B2>(g, w, smem); break;
+        default: run_item<B3>(g, w, smem); break;
+      }
     }
   }
 }
 
+// resident CTAs for the persistent grid (the same for both instantiations: same smem, bounds)
 static int batched_grid(sht_ctx* ctx) {
-  static int per_sm = -1;
-  if (per_sm < 0) {
-    SHT_CUDA(cudaFuncSetAttribute(k_batched, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kBatchedSmem));
-    SHT_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_batched, 128, kBatchedSmem));
-    if (per_sm < 1) per_sm = 1;
-  }
+  static std::once_flag once;
+  static int per_sm = 1;
+  std::call_once(once, [] {
+    SHT_CUDA(cudaFuncSetAttribute(k_batched<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kBatchedSmem));
+    SHT_CUDA(cudaFuncSetAttribute(k_batched<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kBatchedSmem));
+    int a = 0, b = 0;
+    SHT_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a, k_batched<false>, 128, kBatchedSmem));
+    SHT_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_batched<true>, 128, kBatchedSmem));
+    per_sm = std::max(1, std::min(a, b));
+  });
   return ctx->num_sms * per_sm;
 }
 
@@ -208,7 +245,7 @@ static void launch_batched(sht_plan* p, BatchedArgs& b, cudaStream_t s) {
   if (b.nwork <= 0) return;
   SHT_CUDA(cudaMemsetAsync(b.counter, 0, sizeof(int), s));
   const int grid = std::min<long long>(batched_grid(p->ctx), b.nwork);
-  k_batched<<<grid, 128, kBatchedSmem, s>>>(b);
+  k_batched<false><<<grid, 128, kBatchedSmem, s>>>(b);
   SHT_CUDA(cudaGetLastError());
 }
 
@@ -353,7 +390,8 @@ static void fill_operands(sht_plan* p, BatchedArgs& b) {
   b.Bm = p->mf_b.as<double>(); b.boff = p->mf_boff.as<long long>(); b.bld = p->mf_bld.as<int>();
 }
 
-void batched_execute(sht_plan* p, const SparseArgs& g, long long, cudaStream_t s) {
+// Descriptor of one batched plan's execute (also used by the serving loop).
+static BatchedArgs batched_args(sht_plan* p, const SparseArgs& g) {
   BatchedArgs b{};
   b.mp = g.mp;
   b.sc = g.sc;
@@ -367,6 +405,51 @@ void batched_execute(sht_plan* p, const SparseArgs& g, long long, cudaStream_t s
   std::memcpy(&bb, &g.sc.beta, 8);
   b.nwork = (int)((bb == one) ? p->bwork_touched : p->bwork);
   b.counter = p->d_counter.as<int>();
+  return b;
+}
+
+size_t batched_desc_bytes() { return sizeof(BatchedArgs); }
+
+// resident CTAs per SM of the persistent kernel
+int batched_ctas_per_sm(sht_ctx* ctx) { return batched_grid(ctx) / ctx->num_sms; }
+
+// One persistent launch over the work of several batched executes (the serving loop).  The
+// operands must already be in matrix form (matform_execute).  host_descs: pinned host memory
+// for plans.size() descriptors that the caller keeps unchanged until the launch completes (the
+// upload reads it asynchronously); `descs` and `counter` are allocated on `s` and must be held
+// as long.  ctas_per_sm (1..batched_ctas_per_sm) sets the persistent grid: fewer than the
+// maximum leaves room on every SM for the planning kernels of requests that arrive meanwhile.
+// Returns the number of launch items.
+long long batched_multi_launch(sht_ctx* ctx, const std::vector<sht_plan*>& plans, const std::vector<SparseArgs>& args,
+                               void* host_descs, PoolBuf& descs, PoolBuf& counter, int ctas_per_sm, cudaStream_t s) {
+  DevicePool* pool = ctx->pool.get();
+  BatchedArgs* h = static_cast<BatchedArgs*>(host_descs);
+  long long total = 0;
+  for (size_t i = 0; i < plans.size(); ++i) {
+    h[i] = batched_args(plans[i], args[i]);
+    h[i].first = (int)total;
+    total += h[i].nwork;
+    if (total > (long long)INT32_MAX) fail(SHT_ERR_UNSUPPORTED, "batched launch above 2^31 tiles");
+  }
+  if (total == 0) return 0;
+  descs = PoolBuf(pool, plans.size() * sizeof(BatchedArgs), s);
+  counter = PoolBuf(pool, 256, s);
+  SHT_CUDA(cudaMemcpyAsync(descs.ptr, h, plans.size() * sizeof(BatchedArgs), cudaMemcpyHostToDevice, s));
+  BatchedArgs b = h[0];
+  b.nwork = (int)total;
+  b.counter = counter.as<int>();
+  b.multi = descs.as<BatchedArgs>();
+  b.nmulti = (int)plans.size();
+  SHT_CUDA(cudaMemsetAsync(b.counter, 0, sizeof(int), s));
+  const int per_sm = std::max(1, std::min(ctas_per_sm, batched_ctas_per_sm(ctx)));
+  const int grid = (int)std::min<long long>((long long)ctx->num_sms * per_sm, total);
+  k_batched<true><<<grid, 128, kBatchedSmem, s>>>(b);
+  SHT_CUDA(cudaGetLastError());
+  return total;
+}
+
+void batched_execute(sht_plan* p, const SparseArgs& g, long long, cudaStream_t s) {
+  BatchedArgs b = batched_args(p, g);
   if (!g.sc.alpha_zero) matform_execute(p, g.sc.alpha, s);
   trace("batched: matform kernels", s);
   launch_batched(p, b, s);

@@ -22,23 +22,6 @@ void set_last_error(const std::string& msg) { g_last_error = msg; }
 
 [[noreturn]] void fail(sht_status code, const std::string& msg) { throw Error{code, msg}; }
 
-template <class F>
-static sht_status guard(F&& f) {
-  try {
-    f();
-    return SHT_OK;
-  } catch (const Error& e) {
-    set_last_error(e.msg);
-    return e.code;
-  } catch (const std::bad_alloc&) {
-    set_last_error("host out of memory");
-    return SHT_ERR_OOM;
-  } catch (const std::exception& e) {
-    set_last_error(e.what());
-    return SHT_ERR_INVALID;
-  }
-}
-
 static void need(bool cond, const char* msg) {
   if (!cond) fail(SHT_ERR_INVALID, msg);
 }

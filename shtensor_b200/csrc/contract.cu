@@ -590,15 +590,8 @@ void build_work(sht_plan* p, int TM, int TN, cudaStream_t s) {
   p->work_tn = TN;
 }
 
-void plan_execute(sht_plan* p, double alpha, double beta, cudaStream_t s) {
-  sht_tensor *A = p->A, *B = p->B, *C = p->C;
-  for (sht_tensor* t : {A, B, C}) tensor_touch(t, s);
-  for (PoolBuf* b : {&p->d_pair_a, &p->d_pair_b, &p->d_pstart, &p->d_work, &p->d_bwork, &p->d_counter, &p->mf_a,
-                     &p->mf_b, &p->mf_aoff, &p->mf_boff, &p->mf_ald, &p->mf_bld, &p->mf_ak4})
-    b->use_on(s);
-  for (PoolBuf* b : {&p->sp_a, &p->sp_b, &p->sp_ae, &p->sp_be, &p->sp_aoff, &p->sp_boff, &p->sp_aeoff, &p->sp_beoff,
-                     &p->sp_err})
-    b->use_on(s);
+SparseArgs sparse_args(sht_plan* p, double alpha, double beta) {
+  const sht_tensor *A = p->A, *B = p->B, *C = p->C;
   SparseArgs g{};
   g.mp = p->tmaps;
   g.sc.alpha = alpha;
@@ -610,6 +603,23 @@ void plan_execute(sht_plan* p, double alpha, double beta, cudaStream_t s) {
   g.C = C->d_data.as<double>(); g.offC = C->d_offsets.as<long long>(); g.dimsC = C->d_dims.as<int>();
   g.pair_a = p->d_pair_a.as<int>(); g.pair_b = p->d_pair_b.as<int>(); g.pstart = p->d_pstart.as<int>();
   g.work = p->d_work.as<int2>();
+  return g;
+}
+
+void plan_touch(sht_plan* p, cudaStream_t s) {
+  for (sht_tensor* t : {p->A, p->B, p->C}) tensor_touch(t, s);
+  for (PoolBuf* b : {&p->d_pair_a, &p->d_pair_b, &p->d_pstart, &p->d_work, &p->d_bwork, &p->d_counter, &p->mf_a,
+                     &p->mf_b, &p->mf_aoff, &p->mf_boff, &p->mf_ald, &p->mf_bld, &p->mf_ak4, &p->mf_aitems,
+                     &p->mf_bitems})
+    b->use_on(s);
+  for (PoolBuf* b : {&p->sp_a, &p->sp_b, &p->sp_ae, &p->sp_be, &p->sp_aoff, &p->sp_boff, &p->sp_aeoff, &p->sp_beoff,
+                     &p->sp_err})
+    b->use_on(s);
+}
+
+void plan_execute(sht_plan* p, double alpha, double beta, cudaStream_t s) {
+  plan_touch(p, s);
+  const SparseArgs g = sparse_args(p, alpha, beta);
   uint64_t one;
   const double d1 = 1.0;
   std::memcpy(&one, &d1, 8);

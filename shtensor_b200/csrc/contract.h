@@ -29,6 +29,8 @@ struct sht_plan {
   sht::PoolBuf mf_aoff, mf_boff;    // int64 per block offsets
   sht::PoolBuf mf_ald, mf_bld;      // int32 per block leading dimensions (even)
   sht::PoolBuf mf_ak4;              // int32 per A block contracted extent rounded up to 4
+  sht::PoolBuf mf_aitems, mf_bitems;  // int4 (block, k0, k1, 0) slabs of the matform kernel
+  long long mf_naitems = 0, mf_nbitems = 0;
   long long mf_elems = 0;
   // split path: INT8 slices (K-major rows), row / column exponents, error words
   sht::PoolBuf sp_a, sp_b, sp_ae, sp_be, sp_aoff, sp_boff, sp_aeoff, sp_beoff, sp_err;
@@ -57,6 +59,12 @@ void batched_prepare(sht_plan* p, cudaStream_t s);
 void batched_execute(sht_plan* p, const SparseArgs& g, long long nwork_plain, cudaStream_t s);
 void autotune(sht_plan* p, const char* cache_file, cudaStream_t s);
 void matform_prepare(sht_plan* p, cudaStream_t s);
+size_t batched_desc_bytes();
+int batched_ctas_per_sm(sht_ctx* ctx);
+long long batched_multi_launch(sht_ctx* ctx, const std::vector<sht_plan*>& plans, const std::vector<SparseArgs>& args,
+                               void* host_descs, PoolBuf& descs, PoolBuf& counter, int ctas_per_sm, cudaStream_t s);
+SparseArgs sparse_args(sht_plan* p, double alpha, double beta);
+void plan_touch(sht_plan* p, cudaStream_t s);  // plan buffers and tensors: next used on s
 void split_prepare(sht_plan* p, int S, cudaStream_t s);
 void split_execute(sht_plan* p, const SparseArgs& sa, cudaStream_t s);
 void split_check(sht_plan* p, cudaStream_t s);

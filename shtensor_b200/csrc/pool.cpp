@@ -32,13 +32,13 @@ DevicePool::DevicePool(int device, size_t bytes) {
 }
 
 DevicePool::~DevicePool() {
-  for (auto& kv : chunks_)
-    for (cudaEvent_t ev : kv.second.pending) cudaEventDestroy(ev);
+  chunks_.clear();  // returns every pending event to spare_events_
   for (cudaEvent_t ev : spare_events_) cudaEventDestroy(ev);
   if (base_) cudaFree(base_);
 }
 
 void DevicePool::configure(size_t header, size_t align) {
+  std::lock_guard<std::recursive_mutex> lk(mu_);
   if (chunks_.size() != 1 || !chunks_.begin()->second.free)
     fail(SHT_ERR_STATE, "pool_configure needs an empty pool");
   if (align == 0 || (align & (align - 1))) fail(SHT_ERR_INVALID, "alignment must be a power of two");
@@ -49,23 +49,38 @@ void DevicePool::configure(size_t header, size_t align) {
   free_ = cap_ - header_;
 }
 
-cudaEvent_t DevicePool::take_event() {
-  if (!spare_events_.empty()) {
-    cudaEvent_t e = spare_events_.back();
-    spare_events_.pop_back();
-    return e;
-  }
+// An event recorded on `stream` now, shared by the chunks that cover the freed memory; the
+// handle goes back to spare_events_ when the last of them drops it (always under mu_).
+DevicePool::EventRef DevicePool::record_event(cudaStream_t stream) {
   cudaEvent_t e;
-  SHT_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
-  return e;
+  if (!spare_events_.empty()) {
+    e = spare_events_.back();
+    spare_events_.pop_back();
+  } else {
+    SHT_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+  }
+  const cudaError_t rc = cudaEventRecord(e, stream);
+  if (rc != cudaSuccess) {
+    spare_events_.push_back(e);
+    fail(SHT_ERR_CUDA, std::string("cudaEventRecord in pool free: ") + cudaGetErrorString(rc));
+  }
+  return EventRef(new cudaEvent_t(e), [this](cudaEvent_t* p) {
+    spare_events_.push_back(*p);
+    delete p;
+  });
 }
 
-void DevicePool::wait_pending(Chunk& c, cudaStream_t stream) {
-  for (cudaEvent_t ev : c.pending) {
-    SHT_CUDA(cudaStreamWaitEvent(stream, ev, 0));
-    spare_events_.push_back(ev);
-  }
-  c.pending.clear();
+// Drop duplicate events and events whose work is done: they order nothing any more.  Keeps
+// the lists of long-lived free chunks (the arena's tail) short.
+void DevicePool::prune(std::vector<EventRef>& v) {
+  std::sort(v.begin(), v.end());
+  v.erase(std::unique(v.begin(), v.end()), v.end());
+  v.erase(std::remove_if(v.begin(), v.end(), [](const EventRef& e) { return cudaEventQuery(*e) == cudaSuccess; }),
+          v.end());
+}
+
+void DevicePool::wait_pending(const Chunk& c, cudaStream_t stream) {
+  for (const EventRef& ev : c.pending) SHT_CUDA(cudaStreamWaitEvent(stream, *ev, 0));
 }
 
 bool DevicePool::owns(const void* p) const {
@@ -82,10 +97,12 @@ std::map<size_t, DevicePool::Chunk>::iterator DevicePool::find_data(const void* 
 }
 
 void* DevicePool::allocate(size_t bytes, cudaStream_t stream) {
+  std::lock_guard<std::recursive_mutex> lk(mu_);
   const size_t real = round_up(std::max<size_t>(bytes, 1), align_);
   for (auto it = chunks_.begin(); it != chunks_.end(); ++it) {
     Chunk& c = it->second;
     if (!c.free || c.size < real) continue;
+    prune(c.pending);
     wait_pending(c, stream);
     const size_t diff = c.size - real;
     if (diff <= header_) {
@@ -94,11 +111,13 @@ void* DevicePool::allocate(size_t bytes, cudaStream_t stream) {
     } else {
       Chunk rest;
       rest.size = diff - header_;
-      chunks_[it->first + header_ + real] = rest;
+      rest.pending = c.pending;  // the remainder is still covered by the same frees
+      chunks_[it->first + header_ + real] = std::move(rest);
       c.size = real;
       c.free = false;
       free_ -= real + header_;
     }
+    c.pending.clear();
     return base_ + it->first + header_;
   }
   fail(SHT_ERR_OOM, "device pool is out of memory: requested " + std::to_string(bytes) + " bytes, " +
@@ -106,13 +125,13 @@ void* DevicePool::allocate(size_t bytes, cudaStream_t stream) {
 }
 
 void DevicePool::free(void* p, cudaStream_t stream) {
+  std::lock_guard<std::recursive_mutex> lk(mu_);
   if (!p) return;
   auto it = find_data(p);
   Chunk& c = it->second;
+  EventRef ev = record_event(stream);
   c.free = true;
-  cudaEvent_t ev = take_event();
-  SHT_CUDA(cudaEventRecord(ev, stream));
-  c.pending.push_back(ev);
+  c.pending.push_back(std::move(ev));
   free_ += c.size;
   auto nx = std::next(it);
   if (nx != chunks_.end() && nx->second.free) {
@@ -126,13 +145,17 @@ void DevicePool::free(void* p, cudaStream_t stream) {
     if (pv->second.free) {
       pv->second.size += header_ + c.size;
       pv->second.pending.insert(pv->second.pending.end(), c.pending.begin(), c.pending.end());
+      prune(pv->second.pending);
       chunks_.erase(it);
       free_ += header_;
+      return;
     }
   }
+  prune(c.pending);
 }
 
 size_t DevicePool::size_of(void* p) const {
+  std::lock_guard<std::recursive_mutex> lk(mu_);
   auto self = const_cast<DevicePool*>(this);
   return self->find_data(p)->second.size;
 }
@@ -141,6 +164,7 @@ size_t DevicePool::size_of(void* p) const {
 // hand the tail to a free neighbour or a new free chunk; grow in place into a free right
 // neighbour when it is large enough; otherwise allocate, copy on `stream`, free the old one.
 void* DevicePool::reallocate(void* p, size_t bytes, cudaStream_t stream) {
+  std::lock_guard<std::recursive_mutex> lk(mu_);
   if (!p) return allocate(bytes, stream);
   auto it = find_data(p);
   Chunk& c = it->second;
@@ -153,12 +177,14 @@ void* DevicePool::reallocate(void* p, size_t bytes, cudaStream_t stream) {
       Chunk moved = std::move(nx->second);
       chunks_.erase(nx);
       moved.size += diff;
+      moved.pending.push_back(record_event(stream));  // the tail was in use on `stream`
       c.size = real;
       chunks_[it->first + header_ + real] = std::move(moved);
       free_ += diff;
     } else if (diff > header_) {
       Chunk rest;
       rest.size = diff - header_;
+      rest.pending.push_back(record_event(stream));
       c.size = real;
       chunks_[it->first + header_ + real] = std::move(rest);
       free_ += diff - header_;
@@ -169,10 +195,12 @@ void* DevicePool::reallocate(void* p, size_t bytes, cudaStream_t stream) {
   if (nx != chunks_.end() && nx->second.free && header_ + nx->second.size >= need) {
     wait_pending(nx->second, stream);
     const size_t left = header_ + nx->second.size - need;  // bytes of the neighbour left over
+    std::vector<EventRef> nx_pending = std::move(nx->second.pending);
     chunks_.erase(nx);
     if (left >= header_ + align_) {
       Chunk rest;
       rest.size = left - header_;
+      rest.pending = std::move(nx_pending);
       c.size = real;
       chunks_[it->first + header_ + real] = std::move(rest);
       free_ -= need;

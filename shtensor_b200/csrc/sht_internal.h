@@ -3,10 +3,14 @@
 
 #include <cuda_runtime.h>
 
+#include <atomic>
 #include <cstdint>
 #include <cstdio>
+#include <exception>
 #include <map>
 #include <memory>
+#include <mutex>
+#include <new>
 #include <string>
 #include <vector>
 
@@ -26,6 +30,24 @@ struct Error {
 [[noreturn]] void fail(sht_status code, const std::string& msg);
 void set_last_error(const std::string& msg);
 
+// runs f, turning whatever it throws into a status and the calling thread's message
+template <class F>
+sht_status guard(F&& f) {
+  try {
+    f();
+    return SHT_OK;
+  } catch (const Error& e) {
+    set_last_error(e.msg);
+    return e.code;
+  } catch (const std::bad_alloc&) {
+    set_last_error("host out of memory");
+    return SHT_ERR_OOM;
+  } catch (const std::exception& e) {
+    set_last_error(e.what());
+    return SHT_ERR_INVALID;
+  }
+}
+
 #define SHT_CUDA(call)                                                                    \
   do {                                                                                    \
     cudaError_t e_ = (call);                                                              \
@@ -40,7 +62,10 @@ inline cudaStream_t as_stream(void* s) { return reinterpret_cast<cudaStream_t>(s
 // accounting of the reference's MemoryPool (src/Shmem/MemoryPool.h:126-354): each chunk
 // costs `header` bytes, data sizes are rounded up to `align`, frees coalesce both sides.
 // Frees are stream-ordered: a freed chunk carries the event recorded on the freeing stream
-// and the next allocation from it makes its own stream wait on that event.
+// and the next allocation from it makes its own stream wait on that event.  Every piece of
+// a split or merged free chunk keeps the events of the memory it covers (events are shared
+// and recycled when the last chunk holding them is handed out), so memory freed on one
+// stream is never reused on another before the freeing stream's work is done.
 // ---------------------------------------------------------------------------------------
 class DevicePool {
  public:
@@ -51,25 +76,32 @@ class DevicePool {
   void* reallocate(void* p, size_t bytes, cudaStream_t stream);
   size_t size_of(void* p) const;
   size_t capacity() const { return cap_; }
-  size_t free_bytes() const { return free_; }
+  size_t free_bytes() const {
+    std::lock_guard<std::recursive_mutex> lk(mu_);
+    return free_;
+  }
   size_t header() const { return header_; }
   size_t alignment() const { return align_; }
   void configure(size_t header, size_t align);
   bool owns(const void* p) const;
 
  private:
+  using EventRef = std::shared_ptr<cudaEvent_t>;
   struct Chunk {
     size_t size = 0;  // data bytes (header excluded)
     bool free = true;
-    std::vector<cudaEvent_t> pending;
+    std::vector<EventRef> pending;
   };
   // chunk start offset (its header starts here; data at off + header) -> chunk
   std::map<size_t, Chunk> chunks_;
   char* base_ = nullptr;
   size_t cap_ = 0, free_ = 0, header_ = 256, align_ = 256;
   std::vector<cudaEvent_t> spare_events_;
-  cudaEvent_t take_event();
-  void wait_pending(Chunk& c, cudaStream_t stream);
+  // the serving loop allocates from its own thread while callers create tensors
+  mutable std::recursive_mutex mu_;
+  EventRef record_event(cudaStream_t stream);
+  static void prune(std::vector<EventRef>& v);
+  void wait_pending(const Chunk& c, cudaStream_t stream);
   std::map<size_t, Chunk>::iterator find_data(const void* p);
 };
 
@@ -78,9 +110,8 @@ struct PoolBuf {
   DevicePool* pool = nullptr;
   void* ptr = nullptr;
   size_t bytes = 0;
-  cudaStream_t stream = nullptr;
   PoolBuf() = default;
-  PoolBuf(DevicePool* p, size_t b, cudaStream_t s) : pool(p), bytes(b), stream(s) {
+  PoolBuf(DevicePool* p, size_t b, cudaStream_t s) : pool(p), bytes(b), stream_(s) {
     ptr = b ? p->allocate(b, s) : nullptr;
   }
   PoolBuf(const PoolBuf&) = delete;
@@ -89,7 +120,8 @@ struct PoolBuf {
   PoolBuf& operator=(PoolBuf&& o) noexcept {
     if (this != &o) {
       release();
-      pool = o.pool; ptr = o.ptr; bytes = o.bytes; stream = o.stream;
+      pool = o.pool; ptr = o.ptr; bytes = o.bytes;
+      stream_.store(o.stream_.load(std::memory_order_relaxed), std::memory_order_relaxed);
       o.ptr = nullptr; o.bytes = 0;
     }
     return *this;
@@ -98,15 +130,19 @@ struct PoolBuf {
   void release() noexcept {
     // runs in destructors: a failing free (lost CUDA context) leaks instead of terminating
     try {
-      if (ptr && pool) pool->free(ptr, stream);
+      if (ptr && pool) pool->free(ptr, stream_.load(std::memory_order_relaxed));
     } catch (...) {
     }
     ptr = nullptr;
     bytes = 0;
   }
   template <typename T> T* as() const { return static_cast<T*>(ptr); }
-  // the stream whose work must finish before the memory is reused
-  void use_on(cudaStream_t s) { stream = s; }
+  // the stream whose work must finish before the memory is reused (atomic: the serving
+  // loop's planner threads record their streams on shared input tensors concurrently)
+  void use_on(cudaStream_t s) { stream_.store(s, std::memory_order_relaxed); }
+
+ private:
+  std::atomic<cudaStream_t> stream_{nullptr};
 };
 
 }  // namespace sht

@@ -117,61 +117,137 @@ void tensor_sync_host(sht_tensor* t, cudaStream_t s) {
 }
 
 // ---------------------------------------------------------------------------------------
-// Block norms (BlockSpan::get_norm, src/Basics/BlockSpan.h:140-164).  One warp per block.
-// FROBENIUS: lane l accumulates fma(v,v,acc) over elements l, l+32, ... in ascending order,
-// then a shuffle-down tree (16, 8, 4, 2, 1) and a correctly rounded sqrt: a fixed order,
-// so the CPU restatement reproduces it bit for bit.  MAXABS is order-free.  REFCOMPAT
-// evaluates the reference's int accumulator (acc = int(acc + v*v)) sequentially on lane 0.
+// Block norms (BlockSpan::get_norm, src/Basics/BlockSpan.h:140-164).
+// FROBENIUS and MAXABS are evaluated in a fixed order that parallelises within a block, so
+// that a block of millions of elements is spread over many CTAs while the CPU restatement
+// still reproduces the result bit for bit:
+//   the block's n elements are cut into chunks of kNormChunk = 4096 consecutive elements;
+//   in chunk c, lane j (0..127) folds elements c*4096 + j + 128*i, i = 0, 1, ... ascending
+//   (FROBENIUS: p = fma(v, v, p); MAXABS: p = max(p, |v|));
+//   the 128 lane values are halved in place, p[j] op= p[j + h] for h = 64, 32, ..., 1;
+//   the chunk results are folded in ascending chunk order, starting from chunk 0;
+//   FROBENIUS takes a correctly rounded sqrt at the end.
+// REFCOMPAT evaluates the reference's int accumulator (acc = int(acc + v*v)) sequentially,
+// one thread per block, as the reference does.
 // ---------------------------------------------------------------------------------------
+constexpr int kNormChunk = 4096;
+constexpr int kNormLanes = 128;
+
+__global__ void k_norm_chunk_counts(const int* __restrict__ dims, int order, long long n,
+                                    long long* __restrict__ nchunks) {
+  for (long long b = blockIdx.x * (long long)blockDim.x + threadIdx.x; b < n; b += (long long)gridDim.x * blockDim.x) {
+    long long sz = 1;
+    for (int d = 0; d < order; ++d) sz *= dims[b * order + d];
+    nchunks[b] = (sz + kNormChunk - 1) / kNormChunk;
+  }
+}
+
+// one 128-thread CTA per chunk (grid-stride); chunk -> block by binary search on the starts
 template <typename T>
-__global__ void k_block_norms(const T* __restrict__ data, const long long* __restrict__ offsets,
-                              const int* __restrict__ dims, int order, long long n, int norm,
-                              double* __restrict__ out) {
-  const int lane = threadIdx.x & 31;
-  const long long warps = (long long)gridDim.x * (blockDim.x >> 5);
-  for (long long b = blockIdx.x * (long long)(blockDim.x >> 5) + (threadIdx.x >> 5); b < n; b += warps) {
+__global__ void __launch_bounds__(kNormLanes) k_norm_chunks(const T* __restrict__ data,
+                                                            const long long* __restrict__ offsets,
+                                                            const int* __restrict__ dims, int order, long long n,
+                                                            const long long* __restrict__ cstart,
+                                                            const long long* __restrict__ nchunks, int maxabs,
+                                                            double* __restrict__ partial) {
+  __shared__ double red[kNormLanes];
+  const int j = threadIdx.x;
+  const long long total = cstart[n - 1] + nchunks[n - 1];
+  for (long long c = blockIdx.x; c < total; c += gridDim.x) {
+    long long lo = 0, hi = n - 1;  // last block whose first chunk <= c
+    while (lo < hi) {
+      const long long mid = (lo + hi + 1) >> 1;
+      if (cstart[mid] <= c) lo = mid; else hi = mid - 1;
+    }
+    long long sz = 1;
+    for (int d = 0; d < order; ++d) sz *= dims[lo * order + d];
+    const long long base = (c - cstart[lo]) * kNormChunk;
+    const long long end = min(sz, base + kNormChunk);
+    const T* p = data + offsets[lo];
+    double r = 0.0;
+    for (long long e = base + j; e < end; e += kNormLanes) {
+      const double v = (double)p[e];
+      r = maxabs ? fmax(r, fabs(v)) : __fma_rn(v, v, r);
+    }
+    red[j] = r;
+    __syncthreads();
+    for (int h = kNormLanes / 2; h >= 1; h >>= 1) {
+      if (j < h) red[j] = maxabs ? fmax(red[j], red[j + h]) : __dadd_rn(red[j], red[j + h]);
+      __syncthreads();
+    }
+    if (j == 0) partial[c] = red[0];
+    __syncthreads();
+  }
+}
+
+__global__ void k_norm_finish(const long long* __restrict__ cstart, const long long* __restrict__ nchunks, long long n,
+                              const double* __restrict__ partial, int maxabs, double* __restrict__ out) {
+  for (long long b = blockIdx.x * (long long)blockDim.x + threadIdx.x; b < n; b += (long long)gridDim.x * blockDim.x) {
+    const long long c0 = cstart[b], nc = nchunks[b];
+    double r = 0.0;
+    for (long long c = 0; c < nc; ++c) {
+      const double v = partial[c0 + c];
+      r = c == 0 ? v : (maxabs ? fmax(r, v) : __dadd_rn(r, v));
+    }
+    out[b] = maxabs ? r : sqrt(r);
+  }
+}
+
+template <typename T>
+__global__ void k_norm_refcompat(const T* __restrict__ data, const long long* __restrict__ offsets,
+                                 const int* __restrict__ dims, int order, long long n, double* __restrict__ out) {
+  for (long long b = blockIdx.x * (long long)blockDim.x + threadIdx.x; b < n; b += (long long)gridDim.x * blockDim.x) {
     long long sz = 1;
     for (int d = 0; d < order; ++d) sz *= dims[b * order + d];
     const T* p = data + offsets[b];
-    double r = 0.0;
-    if (norm == SHT_NORM_MAXABS) {
-      for (long long e = lane; e < sz; e += 32) r = fmax(r, fabs((double)p[e]));
-#pragma unroll
-      for (int off = 16; off >= 1; off >>= 1) r = fmax(r, __shfl_down_sync(0xffffffffu, r, off));
-    } else if (norm == SHT_NORM_FROBENIUS) {
-      for (long long e = lane; e < sz; e += 32) {
-        const double v = (double)p[e];
-        r = __fma_rn(v, v, r);
-      }
-#pragma unroll
-      for (int off = 16; off >= 1; off >>= 1) r = __dadd_rn(r, __shfl_down_sync(0xffffffffu, r, off));
-      r = sqrt(r);
-    } else {
-      if (lane == 0) {
-        int acc = 0;
-        for (long long e = 0; e < sz; ++e) {
-          const double v = (double)p[e];
-          acc = (int)__dadd_rn((double)acc, __dmul_rn(v, v));
-        }
-        r = sqrt((double)acc);
-      }
+    int acc = 0;
+    for (long long e = 0; e < sz; ++e) {
+      const double v = (double)p[e];
+      acc = (int)__dadd_rn((double)acc, __dmul_rn(v, v));
     }
-    if (lane == 0) out[b] = r;
+    out[b] = sqrt((double)acc);
   }
+}
+
+template <typename T>
+static void norms_typed(sht_tensor* t, sht_norm norm, double* d_out, cudaStream_t s) {
+  const T* data = t->d_data.as<T>();
+  const long long n = t->nblocks;
+  const long long* offs = t->d_offsets.as<long long>();
+  const int* dims = t->d_dims.as<int>();
+  if (norm == SHT_NORM_FROBENIUS_REFCOMPAT) {
+    k_norm_refcompat<T><<<grid_for(n, 128), 128, 0, s>>>(data, offs, dims, t->order, n, d_out);
+    SHT_CUDA(cudaGetLastError());
+    return;
+  }
+  DevicePool* pool = t->ctx->pool.get();
+  PoolBuf cnt(pool, n * 8, s), start(pool, n * 8, s);
+  k_norm_chunk_counts<<<grid_for(n, 256), 256, 0, s>>>(dims, t->order, n, cnt.as<long long>());
+  size_t tb = 0;
+  cub::DeviceScan::ExclusiveSum(nullptr, tb, cnt.as<long long>(), start.as<long long>(), (int)n, s);
+  {
+    PoolBuf tmp(pool, tb, s);
+    cub::DeviceScan::ExclusiveSum(tmp.ptr, tb, cnt.as<long long>(), start.as<long long>(), (int)n, s);
+  }
+  // every block has at most sz/4096 + 1 chunks: the total is bounded without reading it back
+  const long long bound = t->nnz / kNormChunk + n;
+  PoolBuf partial(pool, std::max(bound, 1LL) * 8, s);
+  const int maxabs = norm == SHT_NORM_MAXABS;
+  const int grid = (int)std::min<long long>(bound, (long long)t->ctx->num_sms * 16);
+  k_norm_chunks<T><<<grid, kNormLanes, 0, s>>>(data, offs, dims, t->order, n, start.as<long long>(),
+                                               cnt.as<long long>(), maxabs, partial.as<double>());
+  k_norm_finish<<<grid_for(n, 128), 128, 0, s>>>(start.as<long long>(), cnt.as<long long>(), n,
+                                                 partial.as<double>(), maxabs, d_out);
+  SHT_CUDA(cudaGetLastError());
 }
 
 void tensor_norms_device(sht_tensor* t, sht_norm norm, double* d_out, cudaStream_t s) {
   if (t->nblocks == 0) return;
   tensor_touch(t, s);
-  const int threads = 256;
-  const int grid = grid_for(t->nblocks * 32, threads, t->ctx->num_sms * 16);
   if (t->dtype == SHT_F64)
-    k_block_norms<double><<<grid, threads, 0, s>>>(t->d_data.as<double>(), t->d_offsets.as<long long>(),
-                                                   t->d_dims.as<int>(), t->order, t->nblocks, (int)norm, d_out);
+    norms_typed<double>(t, norm, d_out, s);
   else
-    k_block_norms<float><<<grid, threads, 0, s>>>(t->d_data.as<float>(), t->d_offsets.as<long long>(),
-                                                  t->d_dims.as<int>(), t->order, t->nblocks, (int)norm, d_out);
-  SHT_CUDA(cudaGetLastError());
+    norms_typed<float>(t, norm, d_out, s);
 }
 
 // ---------------------------------------------------------------------------------------

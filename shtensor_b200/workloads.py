@@ -170,3 +170,23 @@ def c3(seed: int = 1, scale: float = 0.125, v_keep: float = 0.1, t_keep: float =
     return Workload("c3", "abcd, cdij -> abij", V, T, empty_tensor([a, b, i, j]), screen_eps=screen_eps,
                     meta={"scale": scale, "v_keep": v_keep, "t_keep": t_keep})
 
+
+
+def c4_request(rng, max_scale: float = 1.0) -> Workload:
+    """One request of the serving mix: a family drawn from c0..c3, its extents scaled by
+    U(0.25, 1) (times ``max_scale``) and, for c0..c2, occupancy drawn from U(0.05, 0.4).
+    c3 keeps its own decay-and-screening sparsity at its default scale times the draw."""
+    fam = int(rng.integers(0, 4))
+    u = float(rng.uniform(0.25, 1.0)) * max_scale
+    occ = float(rng.uniform(0.05, 0.4))
+    seed = int(rng.integers(1, 1 << 30))
+    if fam == 0:
+        w = c0(seed=seed, nblocks=max(2, int(round(20 * u))), p=occ)
+    elif fam == 1:
+        w = c1(seed=seed, scale=u, occupancy=occ)
+    elif fam == 2:
+        w = c2(seed=seed, scale=u, occupancy=occ)
+    else:
+        w = c3(seed=seed, scale=0.125 * u)
+    w.meta.update({"family": w.name, "u": u, "occupancy": occ})
+    return w
