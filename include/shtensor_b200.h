@@ -56,7 +56,7 @@ typedef enum {
 typedef enum { SHT_F32 = 0, SHT_F64 = 1 } sht_dtype;                 /* FloatType, Definitions.h:44-48 */
 typedef enum { SHT_KERNEL_LAPACK = 0, SHT_KERNEL_XMM = 1 } sht_kernel_type; /* KernelType, KernelDefinitions.h:11-15 */
 typedef enum {
-  SHT_NORM_FROBENIUS = 0,            /* sqrt(sum v^2), fixed 32-way strided order */
+  SHT_NORM_FROBENIUS = 0,            /* sqrt(sum v^2) in a fixed chunked order (bit-reproducible) */
   SHT_NORM_MAXABS = 1,
   SHT_NORM_FROBENIUS_REFCOMPAT = 2   /* the reference's int-accumulator evaluation */
 } sht_norm;
@@ -191,7 +191,7 @@ typedef struct {
   int max_active;        /* requests planned or running at once (0 = 64) */
   int max_batch;         /* requests fused into one launch (0 = 32) */
   size_t reserve_bytes;  /* pool bytes that admission leaves free (0 = none) */
-  int planners;          /* planner threads, each with its own stream (0 = 4) */
+  int planners;          /* planner threads, each with its own stream (0 = 8) */
   int ctas_per_sm;       /* persistent CTAs per SM of a serving launch (0 = the most that fit
                             minus one, leaving room for planning kernels) */
 } sht_server_config;

@@ -34,6 +34,9 @@ struct sht_plan {
   long long mf_elems = 0;
   // split path: INT8 slices (K-major rows), row / column exponents, error words
   sht::PoolBuf sp_a, sp_b, sp_ae, sp_be, sp_aoff, sp_boff, sp_aeoff, sp_beoff, sp_err;
+  sht::PoolBuf sp_aitems, sp_bitems;  // int2 (block, first row) items of 32 rows for the slicer
+  long long sp_naitems = 0, sp_nbitems = 0;
+  sht::PoolBuf sp_items, sp_pairs;    // per-tile and per-pair records of the split kernel
   int split_slices = 0;
   // graph replay
   cudaGraph_t graph = nullptr;

@@ -95,7 +95,7 @@ void insert_by_id(std::deque<ReqPtr>& q, ReqPtr r) {
 struct sht_server {
   sht_ctx* ctx = nullptr;
   std::shared_ptr<sht::DevicePool> keep;
-  int max_active = 64, max_batch = 32, nplanners = 4, ctas_per_sm = 0;
+  int max_active = 64, max_batch = 32, nplanners = 8, ctas_per_sm = 0;
   size_t reserve_bytes = 0;
   cudaStream_t exec_stream = nullptr;
   std::vector<cudaStream_t> plan_streams;

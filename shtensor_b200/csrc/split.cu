@@ -7,14 +7,34 @@
 // product is then  C(r,c) = 2^(e_r + f_c) * sum_g 2^(-7g) * P_g(r,c),  P_g = sum_{t+u=g} A_t B_u
 // over g = 2..S+1 (the triangle t+u <= S+1; dropped terms are below the truncation error).
 // Each P_g is an exact INT32 sum, accumulated by tcgen05.mma kind::i8 into its own TMEM
-// columns; the epilogue reads the groups back (tcgen05.ld), combines them in FP64 by Horner's
-// rule from the smallest group up, scales by 2^(e_r+f_c) and adds into FP64 accumulators
-// held in registers, one pair after another in the canonical pair order.  FP64 is used only
-// for the reassembly, the accumulation into C and the scaling exponents.
+// columns; the epilogue reads the groups back (tcgen05.ld), combines them, scales by
+// 2^(e_r+f_c) and adds into FP64 accumulators held in registers, one pair after another in
+// the canonical pair order.  FP64 is used only for the reassembly, the accumulation into C
+// and the scaling exponents.
 //
-// Tile: 128 rows (one TMEM lane per row, M = 128) x 32 columns of one C block; TMEM holds up
-// to 8 groups x 32 columns.  One elected thread issues the MMAs and commits them to an
-// mbarrier; every wait on it is bounded and reports SHT_ERR_TIMEOUT through an error word.
+// Layout.  k_slice writes the slices of every block already in the order the tensor cores
+// read them from shared memory: for A, per 128-row tile and 32-wide k-step, the S slices'
+// 128 x 32-byte slabs one after another, each slab in K-major core matrices (8 rows x 16
+// bytes); B likewise with 32-row (column) tiles.  One k-step of one pair is therefore two
+// contiguous ranges, S*4 KB of A and S*1 KB of B, fetched with two bulk copies
+// (cp.async.bulk, completion counted on an mbarrier).  The B slabs of one k-step lie one
+// after another, so slices u = 1..n together form one operand of 32*n columns.
+//
+// Kernel (k_split, one 576-thread CTA per SM, persistent over 128 x 32 tiles of C):
+//   warp 0      producer: for every (tile, pair, k-step) waits for a free stage of the
+//               4-stage shared-memory ring and issues its two bulk copies;
+//   warp 1      MMA issuer: waits for the stage and issues S MMAs, A slice t times B slices
+//               1..S+1-t (N = 32*(S+1-t)) into TMEM groups t+1..S+1 of one of two
+//               accumulator sets; frees the stage with tcgen05.commit and, at the end of a
+//               pair, commits the accumulator set to the epilogue;
+//   warps 2-17  epilogue: 4 TMEM lane quarters x 4 column quarters of 8 columns; reassemble a
+//               pair's groups while the tensor cores already work on the next pair (second
+//               TMEM set), accumulate in registers, store the tile at the end.
+// Per-tile and per-pair records are built at plan time so that each role reads one record
+// per tile and per pair.  Every wait is bounded: a role that gives up raises a CTA-wide abort
+// flag and the error word (SHT_ERR_TIMEOUT); the others leave their waits on the flag, the
+// MMA issuer drains the tensor core (bounded), the producer waits for its copies in flight
+// (bounded), and TMEM is freed before the CTA exits.
 #include <algorithm>
 #include <cmath>
 #include <cstring>
@@ -26,21 +46,39 @@
 namespace sht {
 
 constexpr int kSplitM = 128, kSplitN = 32, kSplitK = 32, kMaxSlices = 8;
-constexpr int kSplitTmemCols = 256;  // kMaxSlices groups x 32 columns
+constexpr int kSplitStages = 4;
+constexpr int kAChunk = kSplitM * kSplitK;      // bytes of one A slab (128 rows x 32 k)
+constexpr int kBChunk = kSplitN * kSplitK;      // bytes of one B slab (32 columns x 32 k)
+constexpr int kBufCols = kMaxSlices * kSplitN;  // TMEM columns of one accumulator set (8 groups)
+constexpr int kSplitTmemCols = 2 * kBufCols;    // two sets: 512 columns, the whole TMEM of an SM
+constexpr int kEpiWarps = 16;                   // 4 TMEM lane quarters x 4 column quarters
+constexpr int kSplitThreads = 64 + kEpiWarps * 32;
 
 // ------------------------------------------------------------------ slicing
-constexpr int kSliceTab = 4096;
 
-// One CTA per block: row maxima -> exponents, then S int8 slices in K-major rows
-// (out[t][r][k], row length Kp = K rounded up to 32, zero in the K padding).
+// byte offset of (row r, k) inside one K-major slab of 32-byte rows: core matrices of 8 rows
+// x 16 bytes, 128 bytes apart along k (LBO) and 256 bytes apart along rows (SBO)
+__host__ __device__ __forceinline__ int slab_offset(int r, int k) {
+  return (r >> 3) * 256 + (k >> 4) * 128 + (r & 7) * 16 + (k & 15);
+}
+
+// One warp per item of 32 rows of one block (lane = row): the row maximum gives the row's
+// exponent (rows padded up to the tile height R get 0), then the S int8 slices of the row
+// go out in tile order: out[((tile * ksteps + ks) * S + t) * R * 32 + slab_offset(row % R, k)].
+// Rows past the block and k past K are zero.
 __global__ void __launch_bounds__(256) k_slice(const double* __restrict__ src, const long long* __restrict__ src_off,
                                                const int* __restrict__ dims, int order, ModeMap fm, ModeMap km,
                                                const long long* __restrict__ out_off,
                                                const long long* __restrict__ exp_off, signed char* __restrict__ out,
-                                               short* __restrict__ expo, double scale, int S, long long nblocks,
+                                               short* __restrict__ expo, double scale, int S, int R,
+                                               const int2* __restrict__ items, long long nitems,
                                                int* __restrict__ bad) {
-  __shared__ int fo[kSliceTab], ko[kSliceTab];
-  for (long long b = blockIdx.x; b < nblocks; b += gridDim.x) {
+  const int lane = threadIdx.x & 31;
+  const long long nwarps = (long long)gridDim.x * (blockDim.x >> 5);
+  for (long long it = blockIdx.x * (long long)(blockDim.x >> 5) + (threadIdx.x >> 5); it < nitems; it += nwarps) {
+    const int2 item = items[it];
+    const long long b = item.x;
+    const int r = item.y + lane;
     const int* d = dims + b * order;
     int st[kMaxOrder];
     block_strides(d, order, st);
@@ -48,7 +86,7 @@ __global__ void __launch_bounds__(256) k_slice(const double* __restrict__ src, c
     for (int t = 0; t < fm.n; ++t) m *= d[fm.x[t]];
     for (int t = 0; t < km.n; ++t) K *= d[km.x[t]];
     const int Kp = (K + kSplitK - 1) / kSplitK * kSplitK;
-    const bool tab = m <= kSliceTab && K <= kSliceTab;
+    const int ksteps = Kp / kSplitK;
     auto offset = [&](const ModeMap& mm, int idx) {
       int off = 0;
       for (int t = 0; t < mm.n; ++t) {
@@ -58,40 +96,29 @@ __global__ void __launch_bounds__(256) k_slice(const double* __restrict__ src, c
       }
       return off;
     };
-    if (tab) {
-      for (int i = threadIdx.x; i < m; i += blockDim.x) fo[i] = offset(fm, i);
-      for (int i = threadIdx.x; i < K; i += blockDim.x) ko[i] = offset(km, i);
-    }
-    __syncthreads();
     const double* s = src + src_off[b];
-    signed char* o = out + out_off[b];
-    short* ex = expo + exp_off[b];
-    const long long slab = (long long)m * Kp;
-    // pass 1: row exponents (|v| / 2^e < 1), threads over rows
-    for (int r = threadIdx.x; r < m; r += blockDim.x) {
-      const int fr = tab ? fo[r] : offset(fm, r);
-      double mx = 0.0;
+    const bool live = r < m;
+    const int fr = live ? offset(fm, r) : 0;
+    // pass 1: the row exponent (|v| / 2^e < 1)
+    double mx = 0.0;
+    if (live) {
       for (int k = 0; k < K; ++k) {
-        const double v = __dmul_rn(s[fr + (tab ? ko[k] : offset(km, k))], scale);
+        const double v = __dmul_rn(s[fr + offset(km, k)], scale);
         if (!isfinite(v)) atomicExch(bad, 1);
         mx = fmax(mx, fabs(v));
       }
-      int e = 0;
-      if (mx > 0.0) frexp(mx, &e);
-      ex[r] = (short)e;
     }
-    __syncthreads();
-    // pass 2: one thread per (row, 16-wide k chunk), rows fastest across threads
-    const int kq = Kp / 16;
-    for (int it = threadIdx.x; it < m * kq; it += blockDim.x) {
-      const int r = it % m, q = it / m;
-      const int fr = tab ? fo[r] : offset(fm, r);
-      const int e = ex[r];
+    int e = 0;
+    if (mx > 0.0) frexp(mx, &e);
+    expo[exp_off[b] + r] = (short)e;
+    // pass 2: 16 k at a time, S slices of 16 bytes each
+    signed char* o = out + out_off[b] + (long long)(r / R) * ksteps * S * R * kSplitK;
+    for (int q = 0; q < Kp / 16; ++q) {
       signed char pk[kMaxSlices][16];
 #pragma unroll
       for (int j = 0; j < 16; ++j) {
         const int k = q * 16 + j;
-        double x = (k < K) ? scalbn(__dmul_rn(s[fr + (tab ? ko[k] : offset(km, k))], scale), -e) : 0.0;
+        double x = (live && k < K) ? scalbn(__dmul_rn(s[fr + offset(km, k)], scale), -e) : 0.0;
 #pragma unroll
         for (int t = 0; t < kMaxSlices; ++t) {
           const double y = x * 128.0;
@@ -100,10 +127,10 @@ __global__ void __launch_bounds__(256) k_slice(const double* __restrict__ src, c
           x = y - tr;
         }
       }
+      const long long base = (long long)(q / 2) * S * R * kSplitK + slab_offset(r % R, (q & 1) * 16);
       for (int t = 0; t < S; ++t)
-        *reinterpret_cast<int4*>(o + t * slab + (long long)r * Kp + q * 16) = *reinterpret_cast<const int4*>(pk[t]);
+        *reinterpret_cast<int4*>(o + base + (long long)t * R * kSplitK) = *reinterpret_cast<const int4*>(pk[t]);
     }
-    __syncthreads();
   }
 }
 
@@ -117,16 +144,18 @@ __device__ __forceinline__ unsigned long long umma_desc(const void* smem) {
   return a | (8ull << 16) | (16ull << 32) | (1ull << 46);
 }
 
-// kind::i8, signed A and B, S32 accumulate, K-major operands, M = 128, N = 32
-constexpr unsigned kIdescI8 = (2u << 4) | (1u << 7) | (1u << 10) | ((unsigned)(kSplitN >> 3) << 17) |
-                              ((unsigned)(kSplitM >> 4) << 24);
+// kind::i8, signed A and B, S32 accumulate, K-major operands, M = 128, N = n (16..256, % 16)
+__host__ __device__ constexpr unsigned idesc_i8(int n) {
+  return (2u << 4) | (1u << 7) | (1u << 10) | ((unsigned)(n >> 3) << 17) | ((unsigned)(kSplitM >> 4) << 24);
+}
 
-__device__ __forceinline__ void umma_i8(unsigned tmem_d, unsigned long long da, unsigned long long db, int accumulate) {
+__device__ __forceinline__ void umma_i8(unsigned tmem_d, unsigned long long da, unsigned long long db, unsigned idesc,
+                                        int accumulate) {
   asm volatile(
       "{\n\t.reg .pred p;\n\t"
       "setp.ne.b32 p, %4, 0;\n\t"
       "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(tmem_d),
-      "l"(da), "l"(db), "r"(kIdescI8), "r"(accumulate)
+      "l"(da), "l"(db), "r"(idesc), "r"(accumulate)
       : "memory");
 }
 
@@ -139,45 +168,110 @@ __device__ __forceinline__ void mbar_init(void* mbar, unsigned count) {
   asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(mbar)), "r"(count) : "memory");
 }
 
-// bounded wait on an mbarrier phase; returns false on timeout
-__device__ __forceinline__ bool mbar_wait(void* mbar, unsigned parity, long long limit) {
-  const unsigned a = smem_u32(mbar);
-  for (long long i = 0; i < limit; ++i) {
-    unsigned ok;
-    asm volatile(
-        "{\n\t.reg .pred P;\n\t"
-        "mbarrier.try_wait.parity.shared::cta.b64 P, [%1], %2;\n\t"
-        "selp.u32 %0, 1, 0, P;\n\t}\n"
-        : "=r"(ok)
-        : "r"(a), "r"(parity)
-        : "memory");
-    if (ok) return true;
-  }
-  return false;
-}
-
-__device__ __forceinline__ void tmem_ld16(unsigned taddr, unsigned (&v)[16]) {
-  asm volatile(
-      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];\n"
-      : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]), "=r"(v[8]),
-        "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
-      : "r"(taddr)
-      : "memory");
+__device__ __forceinline__ void tmem_ld8(unsigned taddr, unsigned* v) {
+  asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];\n"
+               : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7])
+               : "r"(taddr)
+               : "memory");
 }
 __device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
 __device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
 __device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
-__device__ __forceinline__ void fence_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
 
-__device__ __forceinline__ void cp16(void* smem, const void* gmem, int bytes) {
-  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(smem_u32(smem)), "l"(gmem), "r"(bytes)
+// ------------------------------------------------------------------ mbarrier / bulk copies
+__device__ __forceinline__ bool mbar_try(void* mbar, unsigned parity) {
+  unsigned ok;
+  asm volatile(
+      "{\n\t.reg .pred P;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 P, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, P;\n\t}\n"
+      : "=r"(ok)
+      : "r"(smem_u32(mbar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+
+__device__ __forceinline__ void mbar_arrive(void* mbar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(mbar)) : "memory");
+}
+
+__device__ __forceinline__ void mbar_expect_tx(void* mbar, unsigned bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(mbar)), "r"(bytes) : "memory");
+}
+
+// global -> shared bulk copy (16-byte aligned addresses, size a multiple of 16) completing on mbar
+__device__ __forceinline__ void bulk_g2s(void* smem, const void* gmem, unsigned bytes, void* mbar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                   smem_u32(smem)),
+               "l"(gmem), "r"(bytes), "r"(smem_u32(mbar))
                : "memory");
 }
 
-// int32 -> double with one integer add and one FP64 add: the bits of 1.5*2^52 plus the
-// sign-extended x are the double 1.5*2^52 + x (unit spacing in that binade)
-__device__ __forceinline__ double i2d(unsigned x) {
-  return __longlong_as_double(0x4338000000000000LL + (long long)(int)x) - 6755399441055744.0;
+// int64 -> double for |x| < 2^51 with one integer add and one FP64 add: the bits of
+// 1.5*2^52 plus x are the double 1.5*2^52 + x (unit spacing in that binade), exact
+__device__ __forceinline__ double i2d(long long x) {
+  return __longlong_as_double(0x4338000000000000LL + x) - 6755399441055744.0;
+}
+
+// 2^k as a double for -1022 <= k <= 1023 (exact)
+__device__ __forceinline__ double pow2(int k) { return __longlong_as_double((long long)(k + 1023) << 52); }
+
+// ------------------------------------------------------------------ records
+// The work of one tile (built at plan time): C block and its element offset, row / column
+// tile, pair range and the tile's extents.
+struct SplitItem {
+  long long cbase;
+  int c, rt, ct, pb, pe, mt, nt;
+};
+
+// One block pair (built at plan time): where its slices and exponents start, its k-steps.
+struct SplitPair {
+  long long a_off, b_off, ae_off, be_off;
+  int ksteps, pad;
+};
+
+__global__ void k_split_items(const int4* __restrict__ work, int nwork, const int* __restrict__ pstart,
+                              const long long* __restrict__ offC, const int* __restrict__ dimsC, TileMaps mp,
+                              SplitItem* __restrict__ out) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nwork; i += gridDim.x * blockDim.x) {
+    const int4 w = work[i];
+    const int* cd = dimsC + (long long)w.x * mp.oC;
+    int m = 1, n = 1;
+    for (int q = 0; q < mp.row.n; ++q) m *= cd[mp.row.y[q]];
+    for (int q = 0; q < mp.col.n; ++q) n *= cd[mp.col.y[q]];
+    const int ntr = (m + kSplitM - 1) / kSplitM;
+    SplitItem t;
+    t.cbase = offC[w.x];
+    t.c = w.x;
+    t.rt = w.y % ntr;
+    t.ct = w.y / ntr;
+    t.pb = pstart[w.x];
+    t.pe = pstart[w.x + 1];
+    t.mt = min(kSplitM, m - t.rt * kSplitM);
+    t.nt = min(kSplitN, n - t.ct * kSplitN);
+    out[i] = t;
+  }
+}
+
+__global__ void k_split_pairs(const int* __restrict__ pair_a, const int* __restrict__ pair_b, long long npairs,
+                              const long long* __restrict__ as_off, const long long* __restrict__ bs_off,
+                              const long long* __restrict__ ae_off, const long long* __restrict__ be_off,
+                              const int* __restrict__ dimsA, TileMaps mp, SplitPair* __restrict__ out) {
+  for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < npairs;
+       p += (long long)gridDim.x * blockDim.x) {
+    const int ia = pair_a[p], ib = pair_b[p];
+    const int* ad = dimsA + (long long)ia * mp.oA;
+    int K = 1;
+    for (int q = 0; q < mp.kk.n; ++q) K *= ad[mp.kk.x[q]];
+    SplitPair r;
+    r.a_off = as_off[ia];
+    r.b_off = bs_off[ib];
+    r.ae_off = ae_off[ia];
+    r.be_off = be_off[ib];
+    r.ksteps = (K + kSplitK - 1) / kSplitK;
+    r.pad = 0;
+    out[p] = r;
+  }
 }
 
 // ------------------------------------------------------------------ main kernel
@@ -185,38 +279,40 @@ struct SplitArgs {
   TileMaps mp;
   double beta;
   int beta_zero, alpha_zero, S;
-  const signed char* As; const long long* as_off; const long long* ae_off; const short* Ae;  // A slices
-  const signed char* Bs; const long long* bs_off; const long long* be_off; const short* Be;  // B slices
-  const int* dimsA; const int* dimsB;
-  double* C; const long long* offC; const int* dimsC;
-  const int* pair_a; const int* pair_b; const int* pstart;
-  const int4* work;
+  const signed char* As; const short* Ae;  // A slices and row exponents
+  const signed char* Bs; const short* Be;  // B slices and column exponents
+  double* C; const int* dimsC;
+  const SplitItem* items;  // per work item (tile)
+  const SplitPair* prs;    // per block pair
   int nwork;
-  int* counter;
   int* err;
   long long wait_limit;
 };
 
 struct SplitSmem {
-  union {
-    struct {
-      alignas(128) signed char a[kMaxSlices][kSplitM * kSplitK];  // per slice one 128 x 32 K-major slab
-      alignas(128) signed char b[kMaxSlices][kSplitN * kSplitK];
-    } op;
-    double c[kSplitN][kSplitM + 2];
-  } u;
-  int rowC[kSplitM], colC[kSplitN];
-  short fexp[kSplitN];
-  alignas(8) unsigned long long mbar;
+  alignas(1024) signed char stage[kSplitStages][kMaxSlices * (kAChunk + kBChunk)];
+  alignas(8) unsigned long long full[kSplitStages], empty[kSplitStages], tfull[2], tempty[2], drain;
   unsigned tmem_base;
-  int item;
+  int abort;
 };
 
-__global__ void __launch_bounds__(128, 1) k_split(SplitArgs g) {
-  extern __shared__ __align__(128) unsigned char smem_raw[];
+// bounded wait that also gives up when another role raised the abort flag
+__device__ __forceinline__ bool split_wait(void* mbar, unsigned parity, volatile int* abort, const SplitArgs& g) {
+  for (long long i = 0; i < g.wait_limit; ++i) {
+    if (mbar_try(mbar, parity)) return true;
+    if (*abort) return false;
+  }
+  *abort = 1;
+  atomicExch(g.err, (int)SHT_ERR_TIMEOUT);
+  return false;
+}
+
+__global__ void __launch_bounds__(kSplitThreads, 1) k_split(SplitArgs g) {
+  extern __shared__ __align__(1024) unsigned char smem_raw[];
   SplitSmem& sm = *reinterpret_cast<SplitSmem*>(smem_raw);
-  const int tid = threadIdx.x, warp = tid >> 5;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int S = g.S;
+  volatile int* abort = &sm.abort;
 
   if (warp == 0) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&sm.tmem_base)),
@@ -224,164 +320,213 @@ __global__ void __launch_bounds__(128, 1) k_split(SplitArgs g) {
                  : "memory");
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
   }
-  if (tid == 0) {
-    mbar_init(&sm.mbar, 1);
+  if (tid == 32) {
+    for (int i = 0; i < kSplitStages; ++i) {
+      mbar_init(&sm.full[i], 1);
+      mbar_init(&sm.empty[i], 1);
+    }
+    for (int i = 0; i < 2; ++i) {
+      mbar_init(&sm.tfull[i], 1);
+      mbar_init(&sm.tempty[i], kEpiWarps);
+    }
+    mbar_init(&sm.drain, 1);
+    sm.abort = 0;
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   tc_fence_before();
   __syncthreads();
   tc_fence_after();
   const unsigned tmem = sm.tmem_base;
-  unsigned phase = 0;
-  bool failed = false;
+  const unsigned a_bytes = (unsigned)(S * kAChunk), b_bytes = (unsigned)(S * kBChunk);
 
-  for (;;) {
-    if (tid == 0) sm.item = atomicAdd(g.counter, 1);
-    __syncthreads();
-    const int item = sm.item;
-    __syncthreads();
-    if (item >= g.nwork || failed) break;
-    const int4 w = g.work[item];
-    const int c = w.x;
-    double* cptr = g.C + g.offC[c];
-    const int* cd = g.dimsC + (long long)c * g.mp.oC;
-    int stC[kMaxOrder];
-    block_strides(cd, g.mp.oC, stC);
-    int m = 1, n = 1;
-    for (int t = 0; t < g.mp.row.n; ++t) m *= cd[g.mp.row.y[t]];
-    for (int t = 0; t < g.mp.col.n; ++t) n *= cd[g.mp.col.y[t]];
-    const int ntr = (m + kSplitM - 1) / kSplitM;
-    const int r0 = (w.y % ntr) * kSplitM, c0 = (w.y / ntr) * kSplitN;
-    const int mt = min(kSplitM, m - r0), nt = min(kSplitN, n - c0);
-    for (int i = tid; i < kSplitM + kSplitN; i += 128) {
-      if (i < kSplitM) {
-        int r = r0 + i, off = 0;
-        for (int t = 0; t < g.mp.row.n; ++t) {
-          const int e = cd[g.mp.row.y[t]];
-          off += (r % e) * stC[g.mp.row.y[t]];
+  if (warp == 0) {
+    // ---------------------------------------------------------------- producer
+    if (lane == 0) {
+      long long n = 0;
+      bool ok = true;
+      for (int item = blockIdx.x; ok && item < g.nwork; item += gridDim.x) {
+        const SplitItem t = g.items[item];
+        const int pe = g.alpha_zero ? t.pb : t.pe;
+        for (int p = t.pb; ok && p < pe; ++p) {
+          const SplitPair pr = g.prs[p];
+          const int ksteps = pr.ksteps;
+          const signed char* asrc = g.As + pr.a_off + (long long)t.rt * ksteps * a_bytes;
+          const signed char* bsrc = g.Bs + pr.b_off + (long long)t.ct * ksteps * b_bytes;
+          for (int ks = 0; ks < ksteps; ++ks, ++n) {
+            const int st = (int)(n % kSplitStages);
+            const unsigned ph = (unsigned)((n / kSplitStages) & 1);
+            if (!split_wait(&sm.empty[st], ph ^ 1u, abort, g)) { ok = false; break; }
+            mbar_expect_tx(&sm.full[st], a_bytes + b_bytes);
+            bulk_g2s(sm.stage[st], asrc + (long long)ks * a_bytes, a_bytes, &sm.full[st]);
+            bulk_g2s(sm.stage[st] + a_bytes, bsrc + (long long)ks * b_bytes, b_bytes, &sm.full[st]);
+          }
+        }
+      }
+      if (!ok) {
+        // copies still in flight write into this CTA's shared memory: wait for them (bounded)
+        for (long long j = n > kSplitStages ? n - kSplitStages : 0; j < n; ++j) {
+          const int st = (int)(j % kSplitStages);
+          for (long long i = 0; i < g.wait_limit; ++i)
+            if (mbar_try(&sm.full[st], (unsigned)((j / kSplitStages) & 1))) break;
+        }
+      }
+    }
+    __syncwarp();
+  } else if (warp == 1) {
+    // ---------------------------------------------------------------- MMA issuer
+    if (lane == 0) {
+      long long n = 0, q = 0;
+      bool ok = true;
+      for (int item = blockIdx.x; ok && item < g.nwork; item += gridDim.x) {
+        const SplitItem t = g.items[item];
+        const int pe = g.alpha_zero ? t.pb : t.pe;
+        for (int p = t.pb; ok && p < pe; ++p, ++q) {
+          const int ksteps = g.prs[p].ksteps;
+          const int buf = (int)(q & 1);
+          if (!split_wait(&sm.tempty[buf], (unsigned)(((q >> 1) & 1) ^ 1), abort, g)) { ok = false; break; }
+          tc_fence_after();
+          const unsigned dbase = tmem + (unsigned)(buf * kBufCols);
+          for (int ks = 0; ks < ksteps; ++ks, ++n) {
+            const int st = (int)(n % kSplitStages);
+            if (!split_wait(&sm.full[st], (unsigned)((n / kSplitStages) & 1), abort, g)) { ok = false; break; }
+            tc_fence_after();
+            const signed char* a = sm.stage[st];
+            const signed char* b = sm.stage[st] + a_bytes;
+            // A slice t times B slices 1..S+1-t in one MMA: the products land in TMEM groups
+            // g = t+1 .. S+1, i.e. columns from (t-1)*32 on; t = 1 writes every group first.
+            for (int t = 1; t <= S; ++t) {
+              const int nn = kSplitN * (S + 1 - t);
+              umma_i8(dbase + (unsigned)((t - 1) * kSplitN), umma_desc(a + (t - 1) * kAChunk), umma_desc(b),
+                      idesc_i8(nn), (t == 1 && ks == 0) ? 0 : 1);
+            }
+            umma_commit(&sm.empty[st]);  // the stage is free once these MMAs have read it
+          }
+          if (!ok) break;
+          umma_commit(&sm.tfull[buf]);  // the pair's groups are complete
+        }
+      }
+      // drain: every MMA issued above has finished before TMEM is released (bounded)
+      umma_commit(&sm.drain);
+      for (long long i = 0; i < g.wait_limit; ++i)
+        if (mbar_try(&sm.drain, 0)) break;
+    }
+    __syncwarp();
+  } else {
+    // ---------------------------------------------------------------- epilogue
+    // Per pair, element (r, c) = 2^(e_r + f_c) * sum_{g=2..S+1} 2^(-7g) P_g.  The INT32 groups
+    // are combined exactly in int64 three at a time (P_g 2^14 + P_{g+1} 2^7 + P_{g+2} < 2^46),
+    // each triple is converted once and weighted by an exact power of two, and the scale and
+    // the accumulation are one FMA.
+    const int quarter = warp & 3, cq = (warp - 2) >> 2;
+    const int row = quarter * 32 + lane;  // the TMEM lane this warp may read
+    const unsigned tlane = (unsigned)(quarter * 32) << 16;
+    long long q = 0;
+    bool ok = true;
+    for (int item = blockIdx.x; ok && item < g.nwork; item += gridDim.x) {
+      const SplitItem t = g.items[item];
+      double* cptr = g.C + t.cbase;
+      const int* cd = g.dimsC + (long long)t.c * g.mp.oC;
+      int stC[kMaxOrder];
+      block_strides(cd, g.mp.oC, stC);
+      const int r0 = t.rt * kSplitM, c0 = t.ct * kSplitN + cq * 8;
+      int roff = 0;
+      {
+        int r = r0 + row;
+        for (int x = 0; x < g.mp.row.n; ++x) {
+          const int e = cd[g.mp.row.y[x]];
+          roff += (r % e) * stC[g.mp.row.y[x]];
           r /= e;
         }
-        sm.rowC[i] = (i < mt) ? off : 0;
-      } else {
-        const int j = i - kSplitM;
-        int cc = c0 + j, off = 0;
-        for (int t = 0; t < g.mp.col.n; ++t) {
-          const int e = cd[g.mp.col.y[t]];
-          off += (cc % e) * stC[g.mp.col.y[t]];
-          cc /= e;
-        }
-        sm.colC[j] = (j < nt) ? off : 0;
       }
-    }
-    __syncthreads();
-    // this thread owns tile row `tid` (TMEM lane tid) and all 32 columns
-    double acc[kSplitN];
-    if (g.beta_zero) {
-#pragma unroll
-      for (int j = 0; j < kSplitN; ++j) acc[j] = 0.0;
-    } else {
-      for (int e = tid; e < kSplitM * kSplitN; e += 128) {
-        const int i = e % kSplitM, j = e / kSplitM;
-        sm.u.c[j][i] = (i < mt && j < nt) ? cptr[sm.rowC[i] + sm.colC[j]] : 0.0;
-      }
-      __syncthreads();
-#pragma unroll
-      for (int j = 0; j < kSplitN; ++j) acc[j] = __dmul_rn(g.beta, sm.u.c[j][tid]);
-      __syncthreads();
-    }
-
-    const int pb = g.pstart[c], pe = g.pstart[c + 1];
-    for (int p = pb; p < pe && !g.alpha_zero; ++p) {
-      const int ia = g.pair_a[p], ib = g.pair_b[p];
-      const int* ad = g.dimsA + (long long)ia * g.mp.oA;
-      const int* bdm = g.dimsB + (long long)ib * g.mp.oB;
-      int ma = 1, nb = 1, K = 1;
-      for (int t = 0; t < g.mp.row.n; ++t) ma *= ad[g.mp.row.x[t]];
-      for (int t = 0; t < g.mp.col.n; ++t) nb *= bdm[g.mp.col.x[t]];
-      for (int t = 0; t < g.mp.kk.n; ++t) K *= ad[g.mp.kk.x[t]];
-      const int Kp = (K + kSplitK - 1) / kSplitK * kSplitK;
-      const signed char* abase = g.As + g.as_off[ia];
-      const signed char* bbase = g.Bs + g.bs_off[ib];
-      const long long aslab = (long long)ma * Kp, bslab = (long long)nb * Kp;
-      for (int j = tid; j < kSplitN; j += 128) sm.fexp[j] = (j < nt) ? g.Be[g.be_off[ib] + c0 + j] : 0;
-      const int er = (tid < mt) ? g.Ae[g.ae_off[ia] + r0 + tid] : 0;
-      for (int ks = 0; ks < Kp; ks += kSplitK) {
-        // operand slabs: A rows r0.. (zero past m), B columns c0.. (zero past n)
-        for (int e = tid; e < S * kSplitM * 2; e += 128) {
-          const int t = e / (kSplitM * 2), rem = e % (kSplitM * 2), r = rem >> 1, h = rem & 1;
-          const bool ok = r < mt;
-          const signed char* src = abase + t * aslab + (long long)(ok ? r0 + r : 0) * Kp + ks + h * 16;
-          cp16(&sm.u.op.a[t][(r >> 3) * 256 + h * 128 + (r & 7) * 16], src, ok ? 16 : 0);
+      // column offsets: decompose c0 once, then step the mixed-radix index by one per column
+      int coff[8];
+      {
+        int idx[kMaxOrder], ext[kMaxOrder], str[kMaxOrder];
+        int cc = c0, off = 0;
+        const int nm = g.mp.col.n;
+        for (int x = 0; x < nm; ++x) {
+          ext[x] = cd[g.mp.col.y[x]];
+          str[x] = stC[g.mp.col.y[x]];
+          idx[x] = cc % ext[x];
+          cc /= ext[x];
+          off += idx[x] * str[x];
         }
-        for (int e = tid; e < S * kSplitN * 2; e += 128) {
-          const int t = e / (kSplitN * 2), rem = e % (kSplitN * 2), r = rem >> 1, h = rem & 1;
-          const bool ok = r < nt;
-          const signed char* src = bbase + t * bslab + (long long)(ok ? c0 + r : 0) * Kp + ks + h * 16;
-          cp16(&sm.u.op.b[t][(r >> 3) * 256 + h * 128 + (r & 7) * 16], src, ok ? 16 : 0);
-        }
-        asm volatile("cp.async.commit_group;\ncp.async.wait_group 0;\n" ::: "memory");
-        fence_async_smem();
-        tc_fence_before();
-        __syncthreads();
-        tc_fence_after();
-        if (tid == 0) {
-          for (int gi = 2; gi <= S + 1; ++gi) {
-            const unsigned dcol = tmem + (unsigned)((gi - 2) * kSplitN);
-            bool first = (ks == 0);
-            for (int t = 1; t <= S; ++t) {
-              const int u = gi - t;
-              if (u < 1 || u > S) continue;
-              umma_i8(dcol, umma_desc(sm.u.op.a[t - 1]), umma_desc(sm.u.op.b[u - 1]), first ? 0 : 1);
-              first = false;
-            }
+#pragma unroll
+        for (int j = 0; j < 8; ++j) {
+          coff[j] = off;
+          for (int x = 0; x < nm; ++x) {  // off of column c0 + j + 1
+            off += str[x];
+            if (++idx[x] < ext[x]) break;
+            off -= ext[x] * str[x];
+            idx[x] = 0;
           }
-          umma_commit(&sm.mbar);
         }
-        // every thread waits for the MMAs (operands are rewritten next step, TMEM read below)
-        const bool ok = mbar_wait(&sm.mbar, phase, g.wait_limit);
-        phase ^= 1;
-        tc_fence_after();
-        failed = __syncthreads_or(!ok);
-        if (failed) {
-          if (tid == 0) atomicExch(g.err, (int)SHT_ERR_TIMEOUT);
-          // let the tensor core finish before TMEM is released (bounded as well)
-          mbar_wait(&sm.mbar, phase ^ 1, g.wait_limit);
+      }
+      const bool row_in = row < t.mt;
+      double acc[8];
+#pragma unroll
+      for (int j = 0; j < 8; ++j) {
+        const bool in = row_in && cq * 8 + j < t.nt;
+        acc[j] = (g.beta_zero || !in) ? 0.0 : __dmul_rn(g.beta, cptr[roff + coff[j]]);
+      }
+      const int pe = g.alpha_zero ? t.pb : t.pe;
+      for (int p = t.pb; p < pe; ++p, ++q) {
+        const int buf = (int)(q & 1);
+        // exponents of this pair, fetched before the wait so that their latency overlaps it
+        const SplitPair pr = g.prs[p];
+        const int er = g.Ae[pr.ae_off + r0 + row];
+        short fe[8];
+#pragma unroll
+        for (int j = 0; j < 8; ++j) fe[j] = g.Be[pr.be_off + c0 + j];
+        // warp-uniform: the TMEM loads below are .sync.aligned
+        if (!__all_sync(0xffffffffu, split_wait(&sm.tfull[buf], (unsigned)((q >> 1) & 1), abort, g))) {
+          ok = false;
           break;
         }
-      }
-      if (failed) break;
-      // epilogue for the pair: Horner over groups from the smallest weight up, then scale
+        tc_fence_after();
+        const unsigned tb = tmem + tlane + (unsigned)(buf * kBufCols + cq * 8);
+        // triples of groups g = 2+3c .. 4+3c (index gi = g - 2), smallest weights first
+        double part[8];
 #pragma unroll
-      for (int h = 0; h < kSplitN / 16; ++h) {
-        double part[16];
+        for (int j = 0; j < 8; ++j) part[j] = 0.0;
 #pragma unroll
-        for (int j = 0; j < 16; ++j) part[j] = 0.0;
-        for (int gi = S + 1; gi >= 2; --gi) {
-          unsigned v[16];
-          tmem_ld16(tmem + ((unsigned)(warp * 32) << 16) + (unsigned)((gi - 2) * kSplitN + h * 16), v);
+        for (int c = (kMaxSlices - 1) / 3; c >= 0; --c) {
+          const int g0 = 3 * c;
+          if (g0 >= S) continue;
+          const int len = min(3, S - g0);
+          unsigned v[3][8];
+#pragma unroll
+          for (int i = 0; i < 3; ++i)
+            if (i < len) tmem_ld8(tb + (unsigned)((g0 + i) * kSplitN), v[i]);
           tmem_wait_ld();
+          // the triple's lowest group has weight 2^(-7(g0 + len - 1)) relative to group 2
+          const double w = pow2(-7 * (g0 + len - 1));
 #pragma unroll
-          for (int j = 0; j < 16; ++j) part[j] = fma(part[j], 0.0078125, i2d(v[j]));
+          for (int j = 0; j < 8; ++j) {
+            long long x = (int)v[0][j];
+            if (len > 1) x = x * 128 + (int)v[1][j];
+            if (len > 2) x = x * 128 + (int)v[2][j];
+            part[j] = fma(i2d(x), w, part[j]);
+          }
         }
+        // the accumulator set may be overwritten from here on
+        tc_fence_before();
+        __syncwarp();
+        if (lane == 0) mbar_arrive(&sm.tempty[buf]);
 #pragma unroll
-        for (int j = 0; j < 16; ++j) {
-          acc[h * 16 + j] += scalbn(part[j], er + sm.fexp[h * 16 + j] - 14);
+        for (int j = 0; j < 8; ++j) {
+          const int k = er + (int)fe[j] - 14;
+          // 2^k exact when normal; otherwise scale the sum itself (subnormal results round once)
+          acc[j] = (k >= -1022 && k <= 1023) ? fma(part[j], pow2(k), acc[j]) : acc[j] + scalbn(part[j], k);
         }
       }
-      tc_fence_before();
-      __syncthreads();
-      tc_fence_after();
-    }
-    if (failed) break;
-    // stage and store the tile along C's memory order
+      if (!ok) break;
+      if (row_in) {
 #pragma unroll
-    for (int j = 0; j < kSplitN; ++j) sm.u.c[j][tid] = acc[j];
-    __syncthreads();
-    for (int e = tid; e < kSplitM * kSplitN; e += 128) {
-      const int i = e % kSplitM, j = e / kSplitM;
-      if (i < mt && j < nt) cptr[sm.rowC[i] + sm.colC[j]] = sm.u.c[j][i];
+        for (int j = 0; j < 8; ++j)
+          if (cq * 8 + j < t.nt) cptr[roff + coff[j]] = acc[j];
+      }
     }
-    __syncthreads();
   }
   tc_fence_before();
   __syncthreads();
@@ -397,9 +542,12 @@ static ModeMap modes_of(const std::vector<int>& v) {
   return m;
 }
 
+// Per block: byte offset of its slices (tiles of R rows) and offset of its exponents (rows
+// padded to a multiple of R), plus the slicer's items of 32 rows.  Groups hold exact INT32
+// sums of up to S products of |s| <= 127 per k, so K is limited to keep them below 2^31.
 static void slice_layout(const sht_tensor* T, const std::vector<int>& free_modes, const std::vector<int>& k_modes,
-                         int S, std::vector<long long>& off, std::vector<long long>& eoff, long long& total,
-                         long long& etotal) {
+                         int S, int R, std::vector<long long>& off, std::vector<long long>& eoff, long long& total,
+                         long long& etotal, std::vector<int2>& items) {
   const long long n = T->nblocks;
   off.resize(n);
   eoff.resize(n);
@@ -409,12 +557,15 @@ static void slice_layout(const sht_tensor* T, const std::vector<int>& free_modes
     long long m = 1, K = 1;
     for (int ax : free_modes) m *= T->bs[ax][(id / T->gstride[ax]) % T->nblk[ax]];
     for (int ax : k_modes) K *= T->bs[ax][(id / T->gstride[ax]) % T->nblk[ax]];
+    if (K > 16384) fail(SHT_ERR_UNSUPPORTED, "split mode: contracted block extent above 16384");
     const long long Kp = (K + kSplitK - 1) / kSplitK * kSplitK;
-    if ((long long)S * m * Kp >= (1LL << 31)) fail(SHT_ERR_UNSUPPORTED, "block slices above 2^31 bytes");
+    const long long mp = (m + R - 1) / R * R;
+    if ((long long)S * mp * Kp >= (1LL << 31)) fail(SHT_ERR_UNSUPPORTED, "block slices above 2^31 bytes");
     off[b] = total;
     eoff[b] = etotal;
-    total += (long long)S * m * Kp;  // multiple of 32: every block stays 16-byte aligned
-    etotal += m;
+    total += (long long)S * mp * Kp;  // a multiple of 1 KB: every block stays aligned for bulk copies
+    etotal += mp;
+    for (long long r0 = 0; r0 < mp; r0 += 32) items.push_back(make_int2((int)b, (int)r0));
   }
 }
 
@@ -425,9 +576,10 @@ void split_prepare(sht_plan* p, int S, cudaStream_t s) {
   DevicePool* pool = p->ctx->pool.get();
   p->split_slices = S;
   std::vector<long long> ao, ae, bo, be;
+  std::vector<int2> ia, ib;
   long long at, aet, bt, bet;
-  slice_layout(p->A, p->maps.rowA, p->maps.colA, S, ao, ae, at, aet);
-  slice_layout(p->B, p->maps.colB, p->maps.rowB, S, bo, be, bt, bet);
+  slice_layout(p->A, p->maps.rowA, p->maps.colA, S, kSplitM, ao, ae, at, aet, ia);
+  slice_layout(p->B, p->maps.colB, p->maps.rowB, S, kSplitN, bo, be, bt, bet, ib);
   const long long nA = p->A->nblocks, nB = p->B->nblocks;
   p->sp_a = PoolBuf(pool, std::max(at, 16LL), s);
   p->sp_b = PoolBuf(pool, std::max(bt, 16LL), s);
@@ -438,6 +590,14 @@ void split_prepare(sht_plan* p, int S, cudaStream_t s) {
   p->sp_boff = PoolBuf(pool, std::max(nB, 1LL) * 8, s);
   p->sp_beoff = PoolBuf(pool, std::max(nB, 1LL) * 8, s);
   p->sp_err = PoolBuf(pool, 256, s);
+  p->sp_aitems = PoolBuf(pool, std::max<size_t>(ia.size(), 1) * sizeof(int2), s);
+  p->sp_bitems = PoolBuf(pool, std::max<size_t>(ib.size(), 1) * sizeof(int2), s);
+  p->sp_naitems = (long long)ia.size();
+  p->sp_nbitems = (long long)ib.size();
+  if (!ia.empty())
+    SHT_CUDA(cudaMemcpyAsync(p->sp_aitems.ptr, ia.data(), ia.size() * sizeof(int2), cudaMemcpyHostToDevice, s));
+  if (!ib.empty())
+    SHT_CUDA(cudaMemcpyAsync(p->sp_bitems.ptr, ib.data(), ib.size() * sizeof(int2), cudaMemcpyHostToDevice, s));
   if (nA) {
     SHT_CUDA(cudaMemcpyAsync(p->sp_aoff.ptr, ao.data(), nA * 8, cudaMemcpyHostToDevice, s));
     SHT_CUDA(cudaMemcpyAsync(p->sp_aeoff.ptr, ae.data(), nA * 8, cudaMemcpyHostToDevice, s));
@@ -448,42 +608,57 @@ void split_prepare(sht_plan* p, int S, cudaStream_t s) {
   }
   SHT_CUDA(cudaMemsetAsync(p->sp_err.ptr, 0, 256, s));
   SHT_CUDA(cudaStreamSynchronize(s));
-  // work list: 128 x 32 tiles of every C block, heaviest blocks first
+  // work list: 128 x 32 tiles of every C block, heaviest blocks first, with per-tile and
+  // per-pair records so that the kernel reads each with one load
   device_work_list(p, kSplitM, kSplitN, false, s);
-  p->d_counter = PoolBuf(pool, 256, s);
+  p->sp_items = PoolBuf(pool, std::max(p->bwork, 1LL) * sizeof(SplitItem), s);
+  p->sp_pairs = PoolBuf(pool, std::max(p->npairs, 1LL) * sizeof(SplitPair), s);
+  if (p->bwork > 0)
+    k_split_items<<<grid_for(p->bwork, 256), 256, 0, s>>>(p->d_bwork.as<int4>(), (int)p->bwork, p->d_pstart.as<int>(),
+                                                          p->C->d_offsets.as<long long>(), p->C->d_dims.as<int>(),
+                                                          p->tmaps, p->sp_items.as<SplitItem>());
+  if (p->npairs > 0)
+    k_split_pairs<<<grid_for(p->npairs, 256), 256, 0, s>>>(
+        p->d_pair_a.as<int>(), p->d_pair_b.as<int>(), p->npairs, p->sp_aoff.as<long long>(),
+        p->sp_boff.as<long long>(), p->sp_aeoff.as<long long>(), p->sp_beoff.as<long long>(),
+        p->A->d_dims.as<int>(), p->tmaps, p->sp_pairs.as<SplitPair>());
+  SHT_CUDA(cudaGetLastError());
   SHT_CUDA(cudaStreamSynchronize(s));
 }
 
-// Each CTA holds kSplitTmemCols of the SM's 512 TMEM columns for its lifetime, so at most two
-// may be resident on an SM: the launch reserves enough shared memory that a third cannot fit.
-constexpr size_t kSplitSmemLaunch = std::max<size_t>(sizeof(SplitSmem), 100 * 1024);
+// One CTA per SM: it holds all 512 TMEM columns, and its shared memory keeps a second CTA off.
+constexpr size_t kSplitSmemLaunch = sizeof(SplitSmem);
+static_assert(kSplitSmemLaunch > 114 * 1024, "one split CTA per SM");
 
 static int split_grid(sht_ctx* ctx) {
-  static int per_sm = -1;
-  if (per_sm < 0) {
+  static std::once_flag once;
+  static int per_sm = 1;
+  std::call_once(once, [] {
     SHT_CUDA(cudaFuncSetAttribute(k_split, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSplitSmemLaunch));
-    SHT_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_split, 128, kSplitSmemLaunch));
-    if (per_sm > 512 / kSplitTmemCols) fail(SHT_ERR_STATE, "split kernel occupancy exceeds the TMEM budget");
-    per_sm = std::max(per_sm, 1);
-  }
+    int n = 0;
+    SHT_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_split, kSplitThreads, kSplitSmemLaunch));
+    if (n != 1) fail(SHT_ERR_STATE, "split kernel must run one CTA per SM (TMEM budget)");
+    per_sm = n;
+  });
   return ctx->num_sms * per_sm;
 }
 
 void split_execute(sht_plan* p, const SparseArgs& sa, cudaStream_t s) {
-  const long long nA = p->A->nblocks, nB = p->B->nblocks;
   const int S = p->split_slices;
-  const int cap = p->ctx->num_sms * 8;
   if (!sa.sc.alpha_zero) {
-    if (nA)
-      k_slice<<<(int)std::min<long long>(nA, cap), 256, 0, s>>>(
+    const long long cap = (long long)p->ctx->num_sms * 16;
+    if (p->sp_naitems)
+      k_slice<<<(int)std::min((p->sp_naitems + 7) / 8, cap), 256, 0, s>>>(
           p->A->d_data.as<double>(), p->A->d_offsets.as<long long>(), p->A->d_dims.as<int>(), p->A->order,
           modes_of(p->maps.rowA), modes_of(p->maps.colA), p->sp_aoff.as<long long>(), p->sp_aeoff.as<long long>(),
-          p->sp_a.as<signed char>(), p->sp_ae.as<short>(), sa.sc.alpha, S, nA, p->sp_err.as<int>() + 1);
-    if (nB)
-      k_slice<<<(int)std::min<long long>(nB, cap), 256, 0, s>>>(
+          p->sp_a.as<signed char>(), p->sp_ae.as<short>(), sa.sc.alpha, S, kSplitM, p->sp_aitems.as<int2>(),
+          p->sp_naitems, p->sp_err.as<int>() + 1);
+    if (p->sp_nbitems)
+      k_slice<<<(int)std::min((p->sp_nbitems + 7) / 8, cap), 256, 0, s>>>(
           p->B->d_data.as<double>(), p->B->d_offsets.as<long long>(), p->B->d_dims.as<int>(), p->B->order,
           modes_of(p->maps.colB), modes_of(p->maps.rowB), p->sp_boff.as<long long>(), p->sp_beoff.as<long long>(),
-          p->sp_b.as<signed char>(), p->sp_be.as<short>(), 1.0, S, nB, p->sp_err.as<int>() + 1);
+          p->sp_b.as<signed char>(), p->sp_be.as<short>(), 1.0, S, kSplitN, p->sp_bitems.as<int2>(), p->sp_nbitems,
+          p->sp_err.as<int>() + 1);
     SHT_CUDA(cudaGetLastError());
   }
   uint64_t one, bb;
@@ -496,22 +671,20 @@ void split_execute(sht_plan* p, const SparseArgs& sa, cudaStream_t s) {
   g.beta_zero = sa.sc.beta_zero;
   g.alpha_zero = sa.sc.alpha_zero;
   g.S = S;
-  g.As = p->sp_a.as<signed char>(); g.as_off = p->sp_aoff.as<long long>(); g.ae_off = p->sp_aeoff.as<long long>();
+  g.As = p->sp_a.as<signed char>();
   g.Ae = p->sp_ae.as<short>();
-  g.Bs = p->sp_b.as<signed char>(); g.bs_off = p->sp_boff.as<long long>(); g.be_off = p->sp_beoff.as<long long>();
+  g.Bs = p->sp_b.as<signed char>();
   g.Be = p->sp_be.as<short>();
-  g.dimsA = p->A->d_dims.as<int>(); g.dimsB = p->B->d_dims.as<int>();
-  g.C = sa.C; g.offC = sa.offC; g.dimsC = sa.dimsC;
-  g.pair_a = sa.pair_a; g.pair_b = sa.pair_b; g.pstart = sa.pstart;
-  g.work = p->d_bwork.as<int4>();
+  g.C = sa.C;
+  g.dimsC = sa.dimsC;
+  g.items = p->sp_items.as<SplitItem>();
+  g.prs = p->sp_pairs.as<SplitPair>();
   g.nwork = (int)((bb == one) ? p->bwork_touched : p->bwork);
-  g.counter = p->d_counter.as<int>();
   g.err = p->sp_err.as<int>();
-  g.wait_limit = 1LL << 20;
+  g.wait_limit = 1LL << 22;
   if (g.nwork <= 0) return;
-  SHT_CUDA(cudaMemsetAsync(g.counter, 0, sizeof(int), s));
   const int grid = (int)std::min<long long>(split_grid(p->ctx), g.nwork);
-  k_split<<<grid, 128, kSplitSmemLaunch, s>>>(g);
+  k_split<<<grid, kSplitThreads, kSplitSmemLaunch, s>>>(g);
   SHT_CUDA(cudaGetLastError());
 }
 
