@@ -613,7 +613,8 @@ void plan_touch(sht_plan* p, cudaStream_t s) {
                      &p->mf_bitems})
     b->use_on(s);
   for (PoolBuf* b : {&p->sp_a, &p->sp_b, &p->sp_ae, &p->sp_be, &p->sp_aoff, &p->sp_boff, &p->sp_aeoff, &p->sp_beoff,
-                     &p->sp_err, &p->sp_aitems, &p->sp_bitems, &p->sp_items, &p->sp_pairs})
+                     &p->sp_err, &p->sp_aitems, &p->sp_bitems, &p->sp_items, &p->sp_pairs,
+                     &p->sp_rowtab, &p->sp_coltab})
     b->use_on(s);
 }
 

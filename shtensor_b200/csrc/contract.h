@@ -37,6 +37,7 @@ struct sht_plan {
   sht::PoolBuf sp_aitems, sp_bitems;  // int2 (block, first row) items of 32 rows for the slicer
   long long sp_naitems = 0, sp_nbitems = 0;
   sht::PoolBuf sp_items, sp_pairs;    // per-tile and per-pair records of the split kernel
+  sht::PoolBuf sp_rowtab, sp_coltab;  // element offsets of every C row / column in its block
   int split_slices = 0;
   // graph replay
   cudaGraph_t graph = nullptr;

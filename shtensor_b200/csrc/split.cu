@@ -52,6 +52,7 @@ constexpr int kBChunk = kSplitN * kSplitK;      // bytes of one B slab (32 colum
 constexpr int kBufCols = kMaxSlices * kSplitN;  // TMEM columns of one accumulator set (8 groups)
 constexpr int kSplitTmemCols = 2 * kBufCols;    // two sets: 512 columns, the whole TMEM of an SM
 constexpr int kEpiWarps = 16;                   // 4 TMEM lane quarters x 4 column quarters
+constexpr int kTileSlots = 4, kExpSlots = 4;    // depth of the tile-record and exponent rings
 constexpr int kSplitThreads = 64 + kEpiWarps * 32;
 
 // ------------------------------------------------------------------ slicing
@@ -96,6 +97,10 @@ __global__ void __launch_bounds__(256) k_slice(const double* __restrict__ src, c
       }
       return off;
     };
+    // contracted offsets: one contracted mode (the common case) is a plain stride
+    const bool k1 = km.n == 1;
+    const int kst = k1 ? st[km.x[0]] : 0;
+    auto koff = [&](int k) { return k1 ? k * kst : offset(km, k); };
     const double* s = src + src_off[b];
     const bool live = r < m;
     const int fr = live ? offset(fm, r) : 0;
@@ -103,7 +108,7 @@ __global__ void __launch_bounds__(256) k_slice(const double* __restrict__ src, c
     double mx = 0.0;
     if (live) {
       for (int k = 0; k < K; ++k) {
-        const double v = __dmul_rn(s[fr + offset(km, k)], scale);
+        const double v = __dmul_rn(s[fr + koff(k)], scale);
         if (!isfinite(v)) atomicExch(bad, 1);
         mx = fmax(mx, fabs(v));
       }
@@ -111,25 +116,31 @@ __global__ void __launch_bounds__(256) k_slice(const double* __restrict__ src, c
     int e = 0;
     if (mx > 0.0) frexp(mx, &e);
     expo[exp_off[b] + r] = (short)e;
-    // pass 2: 16 k at a time, S slices of 16 bytes each
+    // pass 2: 16 k at a time; the S slices are packed four bytes to a register and stored
+    // as one 16-byte word each
     signed char* o = out + out_off[b] + (long long)(r / R) * ksteps * S * R * kSplitK;
     for (int q = 0; q < Kp / 16; ++q) {
-      signed char pk[kMaxSlices][16];
+      unsigned w[kMaxSlices][4];
+#pragma unroll
+      for (int t = 0; t < kMaxSlices; ++t) w[t][0] = w[t][1] = w[t][2] = w[t][3] = 0u;
 #pragma unroll
       for (int j = 0; j < 16; ++j) {
         const int k = q * 16 + j;
-        double x = (live && k < K) ? scalbn(__dmul_rn(s[fr + offset(km, k)], scale), -e) : 0.0;
+        double x = (live && k < K) ? scalbn(__dmul_rn(s[fr + koff(k)], scale), -e) : 0.0;
 #pragma unroll
         for (int t = 0; t < kMaxSlices; ++t) {
           const double y = x * 128.0;
           const double tr = trunc(y);
-          pk[t][j] = (signed char)(int)tr;
+          w[t][j >> 2] |= ((unsigned)(int)tr & 0xffu) << ((j & 3) * 8);
           x = y - tr;
         }
       }
       const long long base = (long long)(q / 2) * S * R * kSplitK + slab_offset(r % R, (q & 1) * 16);
-      for (int t = 0; t < S; ++t)
-        *reinterpret_cast<int4*>(o + base + (long long)t * R * kSplitK) = *reinterpret_cast<const int4*>(pk[t]);
+#pragma unroll
+      for (int t = 0; t < kMaxSlices; ++t)
+        if (t < S)
+          *reinterpret_cast<int4*>(o + base + (long long)t * R * kSplitK) =
+              make_int4((int)w[t][0], (int)w[t][1], (int)w[t][2], (int)w[t][3]);
     }
   }
 }
@@ -217,12 +228,14 @@ __device__ __forceinline__ double i2d(long long x) {
 __device__ __forceinline__ double pow2(int k) { return __longlong_as_double((long long)(k + 1023) << 52); }
 
 // ------------------------------------------------------------------ records
-// The work of one tile (built at plan time): C block and its element offset, row / column
-// tile, pair range and the tile's extents.
+// The work of one tile (built at plan time): the C block's element offset, where the tile's
+// rows and columns start in the offset tables, its first row and column within the block,
+// its pair range and its extents.
 struct SplitItem {
   long long cbase;
-  int c, rt, ct, pb, pe, mt, nt;
+  int rtab, ctab, r0, c0, pb, pe, mt, nt, pad;
 };
+static_assert(sizeof(SplitItem) == 48, "tile records are bulk-copied in 16-byte units");
 
 // One block pair (built at plan time): where its slices and exponents start, its k-steps.
 struct SplitPair {
@@ -230,8 +243,42 @@ struct SplitPair {
   int ksteps, pad;
 };
 
+// Element offsets, within their C block, of every row and every column of every C block
+// (rows of block c at rowtab[rowbase[c] ..], columns at coltab[colbase[c] ..]).
+__global__ void k_split_offsets(const int* __restrict__ dimsC, long long nc, TileMaps mp,
+                                const long long* __restrict__ rowbase, const long long* __restrict__ colbase,
+                                int* __restrict__ rowtab, int* __restrict__ coltab) {
+  for (long long c = blockIdx.x; c < nc; c += gridDim.x) {
+    const int* cd = dimsC + c * mp.oC;
+    int st[kMaxOrder];
+    block_strides(cd, mp.oC, st);
+    int m = 1, n = 1;
+    for (int q = 0; q < mp.row.n; ++q) m *= cd[mp.row.y[q]];
+    for (int q = 0; q < mp.col.n; ++q) n *= cd[mp.col.y[q]];
+    for (int r = threadIdx.x; r < m; r += blockDim.x) {
+      int x = r, off = 0;
+      for (int q = 0; q < mp.row.n; ++q) {
+        const int e = cd[mp.row.y[q]];
+        off += (x % e) * st[mp.row.y[q]];
+        x /= e;
+      }
+      rowtab[rowbase[c] + r] = off;
+    }
+    for (int j = threadIdx.x; j < n; j += blockDim.x) {
+      int x = j, off = 0;
+      for (int q = 0; q < mp.col.n; ++q) {
+        const int e = cd[mp.col.y[q]];
+        off += (x % e) * st[mp.col.y[q]];
+        x /= e;
+      }
+      coltab[colbase[c] + j] = off;
+    }
+  }
+}
+
 __global__ void k_split_items(const int4* __restrict__ work, int nwork, const int* __restrict__ pstart,
                               const long long* __restrict__ offC, const int* __restrict__ dimsC, TileMaps mp,
+                              const long long* __restrict__ rowbase, const long long* __restrict__ colbase,
                               SplitItem* __restrict__ out) {
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nwork; i += gridDim.x * blockDim.x) {
     const int4 w = work[i];
@@ -242,13 +289,15 @@ __global__ void k_split_items(const int4* __restrict__ work, int nwork, const in
     const int ntr = (m + kSplitM - 1) / kSplitM;
     SplitItem t;
     t.cbase = offC[w.x];
-    t.c = w.x;
-    t.rt = w.y % ntr;
-    t.ct = w.y / ntr;
+    t.r0 = (w.y % ntr) * kSplitM;
+    t.c0 = (w.y / ntr) * kSplitN;
+    t.rtab = (int)(rowbase[w.x] + t.r0);
+    t.ctab = (int)(colbase[w.x] + t.c0);
     t.pb = pstart[w.x];
     t.pe = pstart[w.x + 1];
-    t.mt = min(kSplitM, m - t.rt * kSplitM);
-    t.nt = min(kSplitN, n - t.ct * kSplitN);
+    t.mt = min(kSplitM, m - t.r0);
+    t.nt = min(kSplitN, n - t.c0);
+    t.pad = 0;
     out[i] = t;
   }
 }
@@ -276,12 +325,12 @@ __global__ void k_split_pairs(const int* __restrict__ pair_a, const int* __restr
 
 // ------------------------------------------------------------------ main kernel
 struct SplitArgs {
-  TileMaps mp;
   double beta;
   int beta_zero, alpha_zero, S;
   const signed char* As; const short* Ae;  // A slices and row exponents
   const signed char* Bs; const short* Be;  // B slices and column exponents
-  double* C; const int* dimsC;
+  double* C;
+  const int* rowtab; const int* coltab;  // element offsets of C rows / columns
   const SplitItem* items;  // per work item (tile)
   const SplitPair* prs;    // per block pair
   int nwork;
@@ -289,9 +338,30 @@ struct SplitArgs {
   long long wait_limit;
 };
 
+// Per tile, the producer also copies the tile's record and its row / column offsets into a
+// ring of tile slots, and per pair the A row and B column exponents into a ring of exponent
+// slots, so the epilogue reads nothing from global memory but the C values it scales by beta.
+struct SplitTileSlot {
+  SplitItem rec;
+  int rowoff[kSplitM];
+  int coloff[kSplitN];
+};
+struct SplitExpSlot {
+  short ea[kSplitM];
+  short eb[kSplitN];
+};
+constexpr unsigned kTileSlotBytes = sizeof(SplitTileSlot);
+constexpr unsigned kExpSlotBytes = sizeof(SplitExpSlot);
+static_assert(sizeof(SplitItem) % 16 == 0 && kTileSlotBytes == 48 + 4 * (kSplitM + kSplitN) &&
+                  kExpSlotBytes == 2 * (kSplitM + kSplitN),
+              "slot members are bulk-copy destinations at 16-byte offsets");
+
 struct SplitSmem {
   alignas(1024) signed char stage[kSplitStages][kMaxSlices * (kAChunk + kBChunk)];
+  alignas(16) SplitTileSlot tile[kTileSlots];
+  alignas(16) SplitExpSlot ex[kExpSlots];
   alignas(8) unsigned long long full[kSplitStages], empty[kSplitStages], tfull[2], tempty[2], drain;
+  unsigned long long ifull[kTileSlots], iempty[kTileSlots], efull[kExpSlots], eempty[kExpSlots];
   unsigned tmem_base;
   int abort;
 };
@@ -329,6 +399,14 @@ __global__ void __launch_bounds__(kSplitThreads, 1) k_split(SplitArgs g) {
       mbar_init(&sm.tfull[i], 1);
       mbar_init(&sm.tempty[i], kEpiWarps);
     }
+    for (int i = 0; i < kTileSlots; ++i) {
+      mbar_init(&sm.ifull[i], 1);
+      mbar_init(&sm.iempty[i], kEpiWarps);
+    }
+    for (int i = 0; i < kExpSlots; ++i) {
+      mbar_init(&sm.efull[i], 1);
+      mbar_init(&sm.eempty[i], kEpiWarps);
+    }
     mbar_init(&sm.drain, 1);
     sm.abort = 0;
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
@@ -342,16 +420,27 @@ __global__ void __launch_bounds__(kSplitThreads, 1) k_split(SplitArgs g) {
   if (warp == 0) {
     // ---------------------------------------------------------------- producer
     if (lane == 0) {
-      long long n = 0;
+      long long n = 0, q = 0, ni = 0;
       bool ok = true;
-      for (int item = blockIdx.x; ok && item < g.nwork; item += gridDim.x) {
+      for (int item = blockIdx.x; ok && item < g.nwork; item += gridDim.x, ++ni) {
         const SplitItem t = g.items[item];
+        const int is = (int)(ni % kTileSlots);
+        if (!split_wait(&sm.iempty[is], (unsigned)(((ni / kTileSlots) & 1) ^ 1), abort, g)) { ok = false; break; }
+        mbar_expect_tx(&sm.ifull[is], kTileSlotBytes);
+        bulk_g2s(&sm.tile[is].rec, g.items + item, sizeof(SplitItem), &sm.ifull[is]);
+        bulk_g2s(sm.tile[is].rowoff, g.rowtab + t.rtab, 4 * kSplitM, &sm.ifull[is]);
+        bulk_g2s(sm.tile[is].coloff, g.coltab + t.ctab, 4 * kSplitN, &sm.ifull[is]);
         const int pe = g.alpha_zero ? t.pb : t.pe;
-        for (int p = t.pb; ok && p < pe; ++p) {
+        for (int p = t.pb; ok && p < pe; ++p, ++q) {
           const SplitPair pr = g.prs[p];
+          const int es = (int)(q % kExpSlots);
+          if (!split_wait(&sm.eempty[es], (unsigned)(((q / kExpSlots) & 1) ^ 1), abort, g)) { ok = false; break; }
+          mbar_expect_tx(&sm.efull[es], kExpSlotBytes);
+          bulk_g2s(sm.ex[es].ea, g.Ae + pr.ae_off + t.r0, 2 * kSplitM, &sm.efull[es]);
+          bulk_g2s(sm.ex[es].eb, g.Be + pr.be_off + t.c0, 2 * kSplitN, &sm.efull[es]);
           const int ksteps = pr.ksteps;
-          const signed char* asrc = g.As + pr.a_off + (long long)t.rt * ksteps * a_bytes;
-          const signed char* bsrc = g.Bs + pr.b_off + (long long)t.ct * ksteps * b_bytes;
+          const signed char* asrc = g.As + pr.a_off + (long long)(t.r0 / kSplitM) * ksteps * a_bytes;
+          const signed char* bsrc = g.Bs + pr.b_off + (long long)(t.c0 / kSplitN) * ksteps * b_bytes;
           for (int ks = 0; ks < ksteps; ++ks, ++n) {
             const int st = (int)(n % kSplitStages);
             const unsigned ph = (unsigned)((n / kSplitStages) & 1);
@@ -364,11 +453,16 @@ __global__ void __launch_bounds__(kSplitThreads, 1) k_split(SplitArgs g) {
       }
       if (!ok) {
         // copies still in flight write into this CTA's shared memory: wait for them (bounded)
-        for (long long j = n > kSplitStages ? n - kSplitStages : 0; j < n; ++j) {
-          const int st = (int)(j % kSplitStages);
-          for (long long i = 0; i < g.wait_limit; ++i)
-            if (mbar_try(&sm.full[st], (unsigned)((j / kSplitStages) & 1))) break;
-        }
+        auto settle = [&](unsigned long long* bars, int nbars, long long issued) {
+          for (long long j = issued > nbars ? issued - nbars : 0; j < issued; ++j) {
+            void* bar = &bars[j % nbars];
+            for (long long i = 0; i < g.wait_limit; ++i)
+              if (mbar_try(bar, (unsigned)((j / nbars) & 1))) break;
+          }
+        };
+        settle(sm.full, kSplitStages, n);
+        settle(sm.efull, kExpSlots, q);
+        settle(sm.ifull, kTileSlots, ni);
       }
     }
     __syncwarp();
@@ -413,56 +507,26 @@ __global__ void __launch_bounds__(kSplitThreads, 1) k_split(SplitArgs g) {
     __syncwarp();
   } else {
     // ---------------------------------------------------------------- epilogue
-    // Per pair, element (r, c) = 2^(e_r + f_c) * sum_{g=2..S+1} 2^(-7g) P_g.  The INT32 groups
-    // are combined exactly in int64 three at a time (P_g 2^14 + P_{g+1} 2^7 + P_{g+2} < 2^46),
-    // each triple is converted once and weighted by an exact power of two, and the scale and
-    // the accumulation are one FMA.
     const int quarter = warp & 3, cq = (warp - 2) >> 2;
     const int row = quarter * 32 + lane;  // the TMEM lane this warp may read
     const unsigned tlane = (unsigned)(quarter * 32) << 16;
-    long long q = 0;
+    long long q = 0, ni = 0;
     bool ok = true;
-    for (int item = blockIdx.x; ok && item < g.nwork; item += gridDim.x) {
-      const SplitItem t = g.items[item];
-      double* cptr = g.C + t.cbase;
-      const int* cd = g.dimsC + (long long)t.c * g.mp.oC;
-      int stC[kMaxOrder];
-      block_strides(cd, g.mp.oC, stC);
-      const int r0 = t.rt * kSplitM, c0 = t.ct * kSplitN + cq * 8;
-      int roff = 0;
-      {
-        int r = r0 + row;
-        for (int x = 0; x < g.mp.row.n; ++x) {
-          const int e = cd[g.mp.row.y[x]];
-          roff += (r % e) * stC[g.mp.row.y[x]];
-          r /= e;
-        }
-      }
-      // column offsets: decompose c0 once, then step the mixed-radix index by one per column
-      int coff[8];
-      {
-        int idx[kMaxOrder], ext[kMaxOrder], str[kMaxOrder];
-        int cc = c0, off = 0;
-        const int nm = g.mp.col.n;
-        for (int x = 0; x < nm; ++x) {
-          ext[x] = cd[g.mp.col.y[x]];
-          str[x] = stC[g.mp.col.y[x]];
-          idx[x] = cc % ext[x];
-          cc /= ext[x];
-          off += idx[x] * str[x];
-        }
-#pragma unroll
-        for (int j = 0; j < 8; ++j) {
-          coff[j] = off;
-          for (int x = 0; x < nm; ++x) {  // off of column c0 + j + 1
-            off += str[x];
-            if (++idx[x] < ext[x]) break;
-            off -= ext[x] * str[x];
-            idx[x] = 0;
-          }
-        }
-      }
+    for (int item = blockIdx.x; ok && item < g.nwork; item += gridDim.x, ++ni) {
+      const int is = (int)(ni % kTileSlots);
+      if (!split_wait(&sm.ifull[is], (unsigned)((ni / kTileSlots) & 1), abort, g)) { ok = false; break; }
+      const SplitTileSlot& ts = sm.tile[is];
+      const SplitItem t = ts.rec;
       const bool row_in = row < t.mt;
+      // a warp whose rows or columns all lie outside a partial tile skips the reassembly
+      const bool warp_live = quarter * 32 < t.mt && cq * 8 < t.nt;
+      const int roff = ts.rowoff[row];
+      int coff[8];
+#pragma unroll
+      for (int j = 0; j < 8; ++j) coff[j] = ts.coloff[cq * 8 + j];
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&sm.iempty[is]);
+      double* cptr = g.C + t.cbase;
       double acc[8];
 #pragma unroll
       for (int j = 0; j < 8; ++j) {
@@ -472,52 +536,62 @@ __global__ void __launch_bounds__(kSplitThreads, 1) k_split(SplitArgs g) {
       const int pe = g.alpha_zero ? t.pb : t.pe;
       for (int p = t.pb; p < pe; ++p, ++q) {
         const int buf = (int)(q & 1);
-        // exponents of this pair, fetched before the wait so that their latency overlaps it
-        const SplitPair pr = g.prs[p];
-        const int er = g.Ae[pr.ae_off + r0 + row];
-        short fe[8];
-#pragma unroll
-        for (int j = 0; j < 8; ++j) fe[j] = g.Be[pr.be_off + c0 + j];
+        const int es = (int)(q % kExpSlots);
         // warp-uniform: the TMEM loads below are .sync.aligned
-        if (!__all_sync(0xffffffffu, split_wait(&sm.tfull[buf], (unsigned)((q >> 1) & 1), abort, g))) {
+        if (!__all_sync(0xffffffffu, split_wait(&sm.efull[es], (unsigned)((q / kExpSlots) & 1), abort, g) &&
+                                         split_wait(&sm.tfull[buf], (unsigned)((q >> 1) & 1), abort, g))) {
           ok = false;
           break;
         }
+        const int er = sm.ex[es].ea[row];
+        int fe[8];
+#pragma unroll
+        for (int j = 0; j < 8; ++j) fe[j] = sm.ex[es].eb[cq * 8 + j];
         tc_fence_after();
-        const unsigned tb = tmem + tlane + (unsigned)(buf * kBufCols + cq * 8);
-        // triples of groups g = 2+3c .. 4+3c (index gi = g - 2), smallest weights first
+        // Per pair, element (r, c) = 2^(e_r + f_c) * sum_{g=2..S+1} 2^(-7g) P_g.  The INT32
+        // groups are combined exactly in int64 three at a time (P_g 2^14 + P_{g+1} 2^7 +
+        // P_{g+2} < 2^46), each triple is converted once and weighted by an exact power of
+        // two (smallest weights first), and the scale and the accumulation are one FMA.
         double part[8];
 #pragma unroll
         for (int j = 0; j < 8; ++j) part[j] = 0.0;
+        if (warp_live) {
+          const unsigned tb = tmem + tlane + (unsigned)(buf * kBufCols + cq * 8);
 #pragma unroll
-        for (int c = (kMaxSlices - 1) / 3; c >= 0; --c) {
-          const int g0 = 3 * c;
-          if (g0 >= S) continue;
-          const int len = min(3, S - g0);
-          unsigned v[3][8];
+          for (int c = (kMaxSlices - 1) / 3; c >= 0; --c) {
+            const int g0 = 3 * c;
+            if (g0 >= S) continue;
+            const int len = min(3, S - g0);
+            unsigned v[3][8];
 #pragma unroll
-          for (int i = 0; i < 3; ++i)
-            if (i < len) tmem_ld8(tb + (unsigned)((g0 + i) * kSplitN), v[i]);
-          tmem_wait_ld();
-          // the triple's lowest group has weight 2^(-7(g0 + len - 1)) relative to group 2
-          const double w = pow2(-7 * (g0 + len - 1));
+            for (int i = 0; i < 3; ++i)
+              if (i < len) tmem_ld8(tb + (unsigned)((g0 + i) * kSplitN), v[i]);
+            tmem_wait_ld();
+            // the triple's lowest group has weight 2^(-7(g0 + len - 1)) relative to group 2
+            const double w = pow2(-7 * (g0 + len - 1));
 #pragma unroll
-          for (int j = 0; j < 8; ++j) {
-            long long x = (int)v[0][j];
-            if (len > 1) x = x * 128 + (int)v[1][j];
-            if (len > 2) x = x * 128 + (int)v[2][j];
-            part[j] = fma(i2d(x), w, part[j]);
+            for (int j = 0; j < 8; ++j) {
+              long long x = (int)v[0][j];
+              if (len > 1) x = x * 128 + (int)v[1][j];
+              if (len > 2) x = x * 128 + (int)v[2][j];
+              part[j] = fma(i2d(x), w, part[j]);
+            }
           }
         }
-        // the accumulator set may be overwritten from here on
+        // the accumulator set and the exponent slot may be overwritten from here on
         tc_fence_before();
         __syncwarp();
-        if (lane == 0) mbar_arrive(&sm.tempty[buf]);
+        if (lane == 0) {
+          mbar_arrive(&sm.tempty[buf]);
+          mbar_arrive(&sm.eempty[es]);
+        }
+        if (warp_live) {
 #pragma unroll
-        for (int j = 0; j < 8; ++j) {
-          const int k = er + (int)fe[j] - 14;
-          // 2^k exact when normal; otherwise scale the sum itself (subnormal results round once)
-          acc[j] = (k >= -1022 && k <= 1023) ? fma(part[j], pow2(k), acc[j]) : acc[j] + scalbn(part[j], k);
+          for (int j = 0; j < 8; ++j) {
+            const int k = er + fe[j] - 14;
+            // 2^k exact when normal; otherwise scale the sum itself (subnormal results round once)
+            acc[j] = (k >= -1022 && k <= 1023) ? fma(part[j], pow2(k), acc[j]) : acc[j] + scalbn(part[j], k);
+          }
         }
       }
       if (!ok) break;
@@ -611,12 +685,41 @@ void split_prepare(sht_plan* p, int S, cudaStream_t s) {
   // work list: 128 x 32 tiles of every C block, heaviest blocks first, with per-tile and
   // per-pair records so that the kernel reads each with one load
   device_work_list(p, kSplitM, kSplitN, false, s);
+  // row / column offset tables of the C blocks (C's host index is current after planning)
+  const sht_tensor* C = p->C;
+  const long long nc = C->nblocks;
+  std::vector<long long> rowbase(std::max(nc, 1LL), 0), colbase(std::max(nc, 1LL), 0);
+  long long rtot = 0, ctot = 0;
+  for (long long c = 0; c < nc; ++c) {
+    const int64_t id = C->ids[c];
+    long long m = 1, n = 1;
+    for (int ax : p->maps.rowC) m *= C->bs[ax][(id / C->gstride[ax]) % C->nblk[ax]];
+    for (int ax : p->maps.colC) n *= C->bs[ax][(id / C->gstride[ax]) % C->nblk[ax]];
+    rowbase[c] = rtot;
+    colbase[c] = ctot;
+    rtot += (m + 3) & ~3LL;  // 16-byte aligned starts: the kernel bulk-copies whole tiles
+    ctot += (n + 3) & ~3LL;
+  }
+  if (rtot >= (1LL << 31) || ctot >= (1LL << 31)) fail(SHT_ERR_UNSUPPORTED, "split mode: C row / column tables above 2^31");
+  PoolBuf drb(pool, rowbase.size() * 8, s), dcb(pool, colbase.size() * 8, s);
+  SHT_CUDA(cudaMemcpyAsync(drb.ptr, rowbase.data(), rowbase.size() * 8, cudaMemcpyHostToDevice, s));
+  SHT_CUDA(cudaMemcpyAsync(dcb.ptr, colbase.data(), colbase.size() * 8, cudaMemcpyHostToDevice, s));
+  // a tile reads a full 128 rows / 32 columns: slack past the last block
+  p->sp_rowtab = PoolBuf(pool, (rtot + kSplitM) * 4, s);
+  p->sp_coltab = PoolBuf(pool, (ctot + kSplitN) * 4, s);
+  SHT_CUDA(cudaMemsetAsync(p->sp_rowtab.ptr, 0, (rtot + kSplitM) * 4, s));
+  SHT_CUDA(cudaMemsetAsync(p->sp_coltab.ptr, 0, (ctot + kSplitN) * 4, s));
+  if (nc > 0)
+    k_split_offsets<<<(int)std::min<long long>(nc, (long long)p->ctx->num_sms * 8), 128, 0, s>>>(
+        C->d_dims.as<int>(), nc, p->tmaps, drb.as<long long>(), dcb.as<long long>(), p->sp_rowtab.as<int>(),
+        p->sp_coltab.as<int>());
   p->sp_items = PoolBuf(pool, std::max(p->bwork, 1LL) * sizeof(SplitItem), s);
   p->sp_pairs = PoolBuf(pool, std::max(p->npairs, 1LL) * sizeof(SplitPair), s);
   if (p->bwork > 0)
     k_split_items<<<grid_for(p->bwork, 256), 256, 0, s>>>(p->d_bwork.as<int4>(), (int)p->bwork, p->d_pstart.as<int>(),
                                                           p->C->d_offsets.as<long long>(), p->C->d_dims.as<int>(),
-                                                          p->tmaps, p->sp_items.as<SplitItem>());
+                                                          p->tmaps, drb.as<long long>(), dcb.as<long long>(),
+                                                          p->sp_items.as<SplitItem>());
   if (p->npairs > 0)
     k_split_pairs<<<grid_for(p->npairs, 256), 256, 0, s>>>(
         p->d_pair_a.as<int>(), p->d_pair_b.as<int>(), p->npairs, p->sp_aoff.as<long long>(),
@@ -666,7 +769,6 @@ void split_execute(sht_plan* p, const SparseArgs& sa, cudaStream_t s) {
   std::memcpy(&one, &d1, 8);
   std::memcpy(&bb, &sa.sc.beta, 8);
   SplitArgs g{};
-  g.mp = sa.mp;
   g.beta = sa.sc.beta;
   g.beta_zero = sa.sc.beta_zero;
   g.alpha_zero = sa.sc.alpha_zero;
@@ -676,7 +778,8 @@ void split_execute(sht_plan* p, const SparseArgs& sa, cudaStream_t s) {
   g.Bs = p->sp_b.as<signed char>();
   g.Be = p->sp_be.as<short>();
   g.C = sa.C;
-  g.dimsC = sa.dimsC;
+  g.rowtab = p->sp_rowtab.as<int>();
+  g.coltab = p->sp_coltab.as<int>();
   g.items = p->sp_items.as<SplitItem>();
   g.prs = p->sp_pairs.as<SplitPair>();
   g.nwork = (int)((bb == one) ? p->bwork_touched : p->bwork);
