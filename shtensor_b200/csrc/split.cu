@@ -35,6 +35,8 @@
 // flag and the error word (SHT_ERR_TIMEOUT); the others leave their waits on the flag, the
 // MMA issuer drains the tensor core (bounded), the producer waits for its copies in flight
 // (bounded), and TMEM is freed before the CTA exits.
+#include <cub/cub.cuh>
+
 #include <algorithm>
 #include <cmath>
 #include <cstring>
@@ -273,6 +275,15 @@ __global__ void k_split_offsets(const int* __restrict__ dimsC, long long nc, Til
       }
       coltab[colbase[c] + j] = off;
     }
+  }
+}
+
+// per C block: rows and columns rounded up to 4 (16-byte aligned table starts)
+__global__ void k_round4(const int* __restrict__ cm, const int* __restrict__ cn, long long nc,
+                         long long* __restrict__ rm, long long* __restrict__ rn) {
+  for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < nc; c += (long long)gridDim.x * blockDim.x) {
+    rm[c] = (cm[c] + 3) & ~3;
+    rn[c] = (cn[c] + 3) & ~3;
   }
 }
 
@@ -586,11 +597,22 @@ __global__ void __launch_bounds__(kSplitThreads, 1) k_split(SplitArgs g) {
           mbar_arrive(&sm.eempty[es]);
         }
         if (warp_live) {
+          // 2^(e_r + f_c - 14) as a product of two exact powers of two when both factors and
+          // the product are normal (the common case, decided once per pair and thread);
+          // otherwise each element is scaled on its own (subnormal results round once)
+          bool normal = er >= -500 && er <= 500;
 #pragma unroll
-          for (int j = 0; j < 8; ++j) {
-            const int k = er + fe[j] - 14;
-            // 2^k exact when normal; otherwise scale the sum itself (subnormal results round once)
-            acc[j] = (k >= -1022 && k <= 1023) ? fma(part[j], pow2(k), acc[j]) : acc[j] + scalbn(part[j], k);
+          for (int j = 0; j < 8; ++j) normal = normal && fe[j] >= -500 && fe[j] <= 500;
+          if (normal) {
+            const double sr = pow2(er - 14);
+#pragma unroll
+            for (int j = 0; j < 8; ++j) acc[j] = fma(part[j], sr * pow2(fe[j]), acc[j]);
+          } else {
+#pragma unroll
+            for (int j = 0; j < 8; ++j) {
+              const int k = er + fe[j] - 14;
+              acc[j] = (k >= -1022 && k <= 1023) ? fma(part[j], pow2(k), acc[j]) : acc[j] + scalbn(part[j], k);
+            }
           }
         }
       }
@@ -682,28 +704,38 @@ void split_prepare(sht_plan* p, int S, cudaStream_t s) {
   }
   SHT_CUDA(cudaMemsetAsync(p->sp_err.ptr, 0, 256, s));
   SHT_CUDA(cudaStreamSynchronize(s));
+  trace("split: slice layout", s);
   // work list: 128 x 32 tiles of every C block, heaviest blocks first, with per-tile and
   // per-pair records so that the kernel reads each with one load
   device_work_list(p, kSplitM, kSplitN, false, s);
-  // row / column offset tables of the C blocks (C's host index is current after planning)
+  trace("split: work list", s);
+  // row / column offset tables of the C blocks: starts from a scan of the blocks' row and
+  // column counts (rounded up to 4 so that every tile's slice of a table is 16-byte aligned)
   const sht_tensor* C = p->C;
   const long long nc = C->nblocks;
-  std::vector<long long> rowbase(std::max(nc, 1LL), 0), colbase(std::max(nc, 1LL), 0);
+  PoolBuf drb(pool, std::max(nc, 1LL) * 8, s), dcb(pool, std::max(nc, 1LL) * 8, s);
   long long rtot = 0, ctot = 0;
-  for (long long c = 0; c < nc; ++c) {
-    const int64_t id = C->ids[c];
-    long long m = 1, n = 1;
-    for (int ax : p->maps.rowC) m *= C->bs[ax][(id / C->gstride[ax]) % C->nblk[ax]];
-    for (int ax : p->maps.colC) n *= C->bs[ax][(id / C->gstride[ax]) % C->nblk[ax]];
-    rowbase[c] = rtot;
-    colbase[c] = ctot;
-    rtot += (m + 3) & ~3LL;  // 16-byte aligned starts: the kernel bulk-copies whole tiles
-    ctot += (n + 3) & ~3LL;
+  if (nc > 0) {
+    PoolBuf rm(pool, nc * 8, s), rn(pool, nc * 8, s);
+    k_round4<<<grid_for(nc, 256), 256, 0, s>>>(p->d_cm.as<int>(), p->d_cn.as<int>(), nc, rm.as<long long>(),
+                                               rn.as<long long>());
+    size_t tb = 0;
+    cub::DeviceScan::ExclusiveSum(nullptr, tb, rm.as<long long>(), drb.as<long long>(), (int)nc, s);
+    {
+      PoolBuf tmp(pool, tb, s);
+      cub::DeviceScan::ExclusiveSum(tmp.ptr, tb, rm.as<long long>(), drb.as<long long>(), (int)nc, s);
+      cub::DeviceScan::ExclusiveSum(tmp.ptr, tb, rn.as<long long>(), dcb.as<long long>(), (int)nc, s);
+    }
+    long long h[4];
+    SHT_CUDA(cudaMemcpyAsync(&h[0], drb.as<long long>() + nc - 1, 8, cudaMemcpyDeviceToHost, s));
+    SHT_CUDA(cudaMemcpyAsync(&h[1], rm.as<long long>() + nc - 1, 8, cudaMemcpyDeviceToHost, s));
+    SHT_CUDA(cudaMemcpyAsync(&h[2], dcb.as<long long>() + nc - 1, 8, cudaMemcpyDeviceToHost, s));
+    SHT_CUDA(cudaMemcpyAsync(&h[3], rn.as<long long>() + nc - 1, 8, cudaMemcpyDeviceToHost, s));
+    SHT_CUDA(cudaStreamSynchronize(s));
+    rtot = h[0] + h[1];
+    ctot = h[2] + h[3];
   }
   if (rtot >= (1LL << 31) || ctot >= (1LL << 31)) fail(SHT_ERR_UNSUPPORTED, "split mode: C row / column tables above 2^31");
-  PoolBuf drb(pool, rowbase.size() * 8, s), dcb(pool, colbase.size() * 8, s);
-  SHT_CUDA(cudaMemcpyAsync(drb.ptr, rowbase.data(), rowbase.size() * 8, cudaMemcpyHostToDevice, s));
-  SHT_CUDA(cudaMemcpyAsync(dcb.ptr, colbase.data(), colbase.size() * 8, cudaMemcpyHostToDevice, s));
   // a tile reads a full 128 rows / 32 columns: slack past the last block
   p->sp_rowtab = PoolBuf(pool, (rtot + kSplitM) * 4, s);
   p->sp_coltab = PoolBuf(pool, (ctot + kSplitN) * 4, s);
@@ -713,6 +745,7 @@ void split_prepare(sht_plan* p, int S, cudaStream_t s) {
     k_split_offsets<<<(int)std::min<long long>(nc, (long long)p->ctx->num_sms * 8), 128, 0, s>>>(
         C->d_dims.as<int>(), nc, p->tmaps, drb.as<long long>(), dcb.as<long long>(), p->sp_rowtab.as<int>(),
         p->sp_coltab.as<int>());
+  trace("split: C offset tables", s);
   p->sp_items = PoolBuf(pool, std::max(p->bwork, 1LL) * sizeof(SplitItem), s);
   p->sp_pairs = PoolBuf(pool, std::max(p->npairs, 1LL) * sizeof(SplitPair), s);
   if (p->bwork > 0)
@@ -727,6 +760,7 @@ void split_prepare(sht_plan* p, int S, cudaStream_t s) {
         p->A->d_dims.as<int>(), p->tmaps, p->sp_pairs.as<SplitPair>());
   SHT_CUDA(cudaGetLastError());
   SHT_CUDA(cudaStreamSynchronize(s));
+  trace("split: tile / pair records", s);
 }
 
 // One CTA per SM: it holds all 512 TMEM columns, and its shared memory keeps a second CTA off.
