@@ -388,11 +388,13 @@ __device__ __forceinline__ bool split_wait(void* mbar, unsigned parity, volatile
   return false;
 }
 
+// S (slices per operand) is a template parameter so that the group loops of the MMA issuer
+// and of the reassembly unroll completely; one instance per S = 1..8.
+template <int S>
 __global__ void __launch_bounds__(kSplitThreads, 1) k_split(SplitArgs g) {
   extern __shared__ __align__(1024) unsigned char smem_raw[];
   SplitSmem& sm = *reinterpret_cast<SplitSmem*>(smem_raw);
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  const int S = g.S;
   volatile int* abort = &sm.abort;
 
   if (warp == 0) {
@@ -767,17 +769,21 @@ void split_prepare(sht_plan* p, int S, cudaStream_t s) {
 constexpr size_t kSplitSmemLaunch = sizeof(SplitSmem);
 static_assert(kSplitSmemLaunch > 114 * 1024, "one split CTA per SM");
 
+using SplitKernel = void (*)(SplitArgs);
+static const SplitKernel kSplitKernels[kMaxSlices] = {k_split<1>, k_split<2>, k_split<3>, k_split<4>,
+                                                      k_split<5>, k_split<6>, k_split<7>, k_split<8>};
+
 static int split_grid(sht_ctx* ctx) {
   static std::once_flag once;
-  static int per_sm = 1;
   std::call_once(once, [] {
-    SHT_CUDA(cudaFuncSetAttribute(k_split, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSplitSmemLaunch));
-    int n = 0;
-    SHT_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_split, kSplitThreads, kSplitSmemLaunch));
-    if (n != 1) fail(SHT_ERR_STATE, "split kernel must run one CTA per SM (TMEM budget)");
-    per_sm = n;
+    for (SplitKernel k : kSplitKernels) {
+      SHT_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSplitSmemLaunch));
+      int n = 0;
+      SHT_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k, kSplitThreads, kSplitSmemLaunch));
+      if (n != 1) fail(SHT_ERR_STATE, "split kernel must run one CTA per SM (TMEM budget)");
+    }
   });
-  return ctx->num_sms * per_sm;
+  return ctx->num_sms;
 }
 
 void split_execute(sht_plan* p, const SparseArgs& sa, cudaStream_t s) {
@@ -821,7 +827,7 @@ void split_execute(sht_plan* p, const SparseArgs& sa, cudaStream_t s) {
   g.wait_limit = 1LL << 22;
   if (g.nwork <= 0) return;
   const int grid = (int)std::min<long long>(split_grid(p->ctx), g.nwork);
-  k_split<<<grid, kSplitThreads, kSplitSmemLaunch, s>>>(g);
+  kSplitKernels[S - 1]<<<grid, kSplitThreads, kSplitSmemLaunch, s>>>(g);
   SHT_CUDA(cudaGetLastError());
 }
 
