@@ -560,6 +560,8 @@ __global__ void __launch_bounds__(kSplitThreads, 1) k_split(SplitArgs g) {
         int fe[8];
 #pragma unroll
         for (int j = 0; j < 8; ++j) fe[j] = sm.ex[es].eb[cq * 8 + j];
+        __syncwarp();
+        if (lane == 0) mbar_arrive(&sm.eempty[es]);  // the exponents are in registers
         tc_fence_after();
         // Per pair, element (r, c) = 2^(e_r + f_c) * sum_{g=2..S+1} 2^(-7g) P_g.  The INT32
         // groups are combined exactly in int64 three at a time (P_g 2^14 + P_{g+1} 2^7 +
@@ -580,6 +582,12 @@ __global__ void __launch_bounds__(kSplitThreads, 1) k_split(SplitArgs g) {
             for (int i = 0; i < 3; ++i)
               if (i < len) tmem_ld8(tb + (unsigned)((g0 + i) * kSplitN), v[i]);
             tmem_wait_ld();
+            if (c == 0) {
+              // the last groups are in registers: the accumulator set may be overwritten
+              tc_fence_before();
+              __syncwarp();
+              if (lane == 0) mbar_arrive(&sm.tempty[buf]);
+            }
             // the triple's lowest group has weight 2^(-7(g0 + len - 1)) relative to group 2
             const double w = pow2(-7 * (g0 + len - 1));
 #pragma unroll
@@ -591,12 +599,10 @@ __global__ void __launch_bounds__(kSplitThreads, 1) k_split(SplitArgs g) {
             }
           }
         }
-        // the accumulator set and the exponent slot may be overwritten from here on
-        tc_fence_before();
-        __syncwarp();
-        if (lane == 0) {
-          mbar_arrive(&sm.tempty[buf]);
-          mbar_arrive(&sm.eempty[es]);
+        if (!warp_live) {
+          tc_fence_before();
+          __syncwarp();
+          if (lane == 0) mbar_arrive(&sm.tempty[buf]);
         }
         if (warp_live) {
           // 2^(e_r + f_c - 14) as a product of two exact powers of two when both factors and
