@@ -166,7 +166,8 @@ sht_status sht_autotune(sht_plan* p, const char* cache_file, void* stream);
 sht_status sht_set_split_slices(sht_ctx* ctx, int slices);
 
 /* ---- diagnostics ---- */
-/* which = 0: FP64 FMA peak of this GPU in TFLOP/s (the FP64 kernels' roofline denominator) */
+/* which = 0: FP64 FMA peak of this GPU in TFLOP/s (the FP64 kernels' roofline denominator);
+ * which = 1: dense INT8 tensor-core (tcgen05 kind::i8) peak in TOPS (the split kernel's) */
 sht_status sht_measure_peak(sht_ctx* ctx, int which, double* value);
 
 /* ---- serving loop (no reference counterpart: shtensor has no request loop) ----

@@ -435,9 +435,10 @@ def contract(ctx: Context, expr: str, alpha: float, A: Tensor, B: Tensor, beta: 
 
 
 def measure_peak(ctx: Context, which: str = "fp64") -> float:
-    """Roofline denominators measured on this GPU: 'fp64' = FP64 FMA TFLOP/s."""
+    """Roofline denominators measured on this GPU: 'fp64' = FP64 FMA TFLOP/s, 'int8' = dense
+    INT8 tensor-core TOPS."""
     v = C.c_double()
-    _check(lib().sht_measure_peak(ctx.handle, {"fp64": 0}[which], C.byref(v)))
+    _check(lib().sht_measure_peak(ctx.handle, {"fp64": 0, "int8": 1}[which], C.byref(v)))
     return v.value
 
 

@@ -9,6 +9,7 @@
 namespace sht {
 
 double measure_fp64_tflops(sht_ctx* ctx);
+double measure_int8_tops(sht_ctx* ctx);
 void stack_call_static(sht_kernel* k, const double* a, const double* b, double* c, int64_t nb_ops, cudaStream_t s);
 
 static void prepare_mode(sht_plan* p, cudaStream_t s) {
@@ -477,8 +478,12 @@ sht_status sht_set_split_slices(sht_ctx* ctx, int slices) {
 sht_status sht_measure_peak(sht_ctx* ctx, int which, double* value) {
   return guard([&] {
     need(ctx && value, "null argument");
-    if (which != 0) fail(SHT_ERR_UNSUPPORTED, "unknown peak");
-    *value = measure_fp64_tflops(ctx);
+    if (which == 0)
+      *value = measure_fp64_tflops(ctx);
+    else if (which == 1)
+      *value = measure_int8_tops(ctx);
+    else
+      fail(SHT_ERR_UNSUPPORTED, "unknown peak");
   });
 }
 

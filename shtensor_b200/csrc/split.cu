@@ -837,6 +837,72 @@ void split_execute(sht_plan* p, const SparseArgs& sa, cudaStream_t s) {
   SHT_CUDA(cudaGetLastError());
 }
 
+// ------------------------------------------------------------------ INT8 tensor-core peak
+// Roofline denominator of the split kernel: every SM issues `iters` dense 128 x 256 x 32
+// kind::i8 MMAs from shared memory into one TMEM accumulator (operands are zero) and waits
+// for them with a bounded mbarrier wait; *status is set if a wait expires.
+__global__ void __launch_bounds__(128, 1) k_int8_peak(int iters, long long wait_limit, int* status) {
+  __shared__ __align__(1024) signed char a[kSplitM * kSplitK];
+  __shared__ __align__(1024) signed char b[256 * kSplitK];
+  __shared__ __align__(8) unsigned long long done;
+  __shared__ unsigned tbase;
+  const int tid = threadIdx.x, warp = tid >> 5;
+  for (int i = tid; i < (int)sizeof(a) / 16; i += blockDim.x) reinterpret_cast<int4*>(a)[i] = make_int4(0, 0, 0, 0);
+  for (int i = tid; i < (int)sizeof(b) / 16; i += blockDim.x) reinterpret_cast<int4*>(b)[i] = make_int4(0, 0, 0, 0);
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&tbase)), "r"(256)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  if (tid == 0) {
+    mbar_init(&done, 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const unsigned tmem = tbase;
+  if (tid == 0) {
+    const unsigned long long da = umma_desc(a), db = umma_desc(b);
+    for (int i = 0; i < iters; ++i) umma_i8(tmem, da, db, idesc_i8(256), i > 0 ? 1 : 0);
+    umma_commit(&done);
+    bool ok = false;
+    for (long long i = 0; i < wait_limit && !ok; ++i) ok = mbar_try(&done, 0);
+    if (!ok) atomicExch(status, 1);
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 0)
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(256) : "memory");
+}
+
+double measure_int8_tops(sht_ctx* ctx) {
+  const int iters = 1 << 14;
+  PoolBuf st(ctx->pool.get(), 256, nullptr);
+  SHT_CUDA(cudaMemsetAsync(st.ptr, 0, 4, nullptr));
+  cudaEvent_t e0, e1;
+  SHT_CUDA(cudaEventCreate(&e0));
+  SHT_CUDA(cudaEventCreate(&e1));
+  double best = 0.0;
+  for (int rep = 0; rep < 4; ++rep) {
+    SHT_CUDA(cudaEventRecord(e0, nullptr));
+    k_int8_peak<<<ctx->num_sms, 128, 0, nullptr>>>(iters, 1LL << 24, st.as<int>());
+    SHT_CUDA(cudaEventRecord(e1, nullptr));
+    SHT_CUDA(cudaEventSynchronize(e1));
+    float ms = 0;
+    SHT_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+    const double ops = 2.0 * kSplitM * 256.0 * kSplitK * (double)iters * ctx->num_sms;
+    if (rep > 0) best = std::max(best, ops / (ms * 1e-3) / 1e12);
+  }
+  int status = 0;
+  SHT_CUDA(cudaMemcpy(&status, st.ptr, 4, cudaMemcpyDeviceToHost));
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (status) fail(SHT_ERR_TIMEOUT, "INT8 peak probe: a bounded wait on the tensor cores expired");
+  return best;
+}
+
 // error words of the last split execute: [0] status from bounded waits, [1] non-finite input
 void split_check(sht_plan* p, cudaStream_t s) {
   int e[2] = {0, 0};

@@ -73,3 +73,13 @@ def test_kernel_errors(ctx):
     assert "map_row" in k.get_info()
     with pytest.raises(sht.ShtError):
         k.call(np.zeros(4), np.zeros(4), np.zeros(4), -1)
+
+
+def test_measured_peaks_are_plausible(ctx):
+    # the in-run roofline denominators: FP64 FMA and dense INT8 tensor-core rates of this GPU
+    fp64 = sht.measure_peak(ctx, "fp64")
+    int8 = sht.measure_peak(ctx, "int8")
+    assert 5.0 < fp64 < 200.0, fp64
+    assert 100.0 < int8 < 20000.0, int8
+    v = __import__("ctypes").c_double()
+    assert sht.lib().sht_measure_peak(ctx.handle, 7, __import__("ctypes").byref(v)) == sht.Status.ERR_UNSUPPORTED
