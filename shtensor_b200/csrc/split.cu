@@ -187,6 +187,9 @@ __device__ __forceinline__ void tmem_ld8(unsigned taddr, unsigned* v) {
                : "r"(taddr)
                : "memory");
 }
+// Orders this thread's generic-proxy shared-memory accesses before later async-proxy ones
+// (bulk copies into a buffer it has read).
+__device__ __forceinline__ void fence_proxy_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
 __device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
 __device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
 __device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
@@ -537,6 +540,9 @@ __global__ void __launch_bounds__(kSplitThreads, 1) k_split(SplitArgs g) {
       int coff[8];
 #pragma unroll
       for (int j = 0; j < 8; ++j) coff[j] = ts.coloff[cq * 8 + j];
+      // the slot is refilled by the async proxy (bulk copy): order this warp's generic reads
+      // of it before the release (write-after-read across proxies needs the proxy fence)
+      fence_proxy_async_smem();
       __syncwarp();
       if (lane == 0) mbar_arrive(&sm.iempty[is]);
       double* cptr = g.C + t.cbase;
@@ -560,6 +566,7 @@ __global__ void __launch_bounds__(kSplitThreads, 1) k_split(SplitArgs g) {
         int fe[8];
 #pragma unroll
         for (int j = 0; j < 8; ++j) fe[j] = sm.ex[es].eb[cq * 8 + j];
+        fence_proxy_async_smem();  // as for the tile slot
         __syncwarp();
         if (lane == 0) mbar_arrive(&sm.eempty[es]);  // the exponents are in registers
         tc_fence_after();
