@@ -365,6 +365,7 @@ void device_work_list(sht_plan* p, int fixed_tm, int fixed_tn, bool per_class, c
   SHT_CUDA(cudaMemcpyAsync(&h[1], tsorted.as<long long>() + nc - 1, 8, cudaMemcpyDeviceToHost, s));
   SHT_CUDA(cudaMemcpyAsync(&h[2], sums.ptr, 8, cudaMemcpyDeviceToHost, s));
   SHT_CUDA(cudaStreamSynchronize(s));
+  plan_flops(p, s);  // the stream is idle after the reads above
   const long long total = h[0] + h[1];
   if (total > (long long)INT32_MAX) fail(SHT_ERR_UNSUPPORTED, "work list above 2^31 tiles");
   p->bwork = total;

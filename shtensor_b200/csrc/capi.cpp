@@ -12,6 +12,53 @@ double measure_fp64_tflops(sht_ctx* ctx);
 double measure_int8_tops(sht_ctx* ctx);
 void stack_call_static(sht_kernel* k, const double* a, const double* b, double* c, int64_t nb_ops, cudaStream_t s);
 
+// A lane (stream + two events) borrowed from the context for the length of one call.
+struct LaneLease {
+  sht_ctx* ctx;
+  sht_ctx::Lane lane;
+  explicit LaneLease(sht_ctx* c) : ctx(c) {
+    {
+      std::lock_guard<std::mutex> lk(ctx->lanes_mu);
+      if (!ctx->lanes.empty()) {
+        lane = ctx->lanes.back();
+        ctx->lanes.pop_back();
+        return;
+      }
+    }
+    SHT_CUDA(cudaStreamCreateWithFlags(&lane.stream, cudaStreamNonBlocking));
+    SHT_CUDA(cudaEventCreateWithFlags(&lane.start, cudaEventDisableTiming));
+    SHT_CUDA(cudaEventCreateWithFlags(&lane.done, cudaEventDisableTiming));
+  }
+  ~LaneLease() {
+    // work still queued on the stream stays ordered by the events of whoever uses it next
+    std::lock_guard<std::mutex> lk(ctx->lanes_mu);
+    ctx->lanes.push_back(lane);
+  }
+  LaneLease(const LaneLease&) = delete;
+  LaneLease& operator=(const LaneLease&) = delete;
+};
+
+// Split form of sht_contract with the slicer overlapped: the slices depend on the patterns and
+// values of A and B only, so they run on the caller's stream s while the pair list, result
+// pattern and records are built on a second stream, which first waits for the work already
+// on s (earlier writes of C) and which s waits for before the tensor-core kernel.
+static void contract_split(sht_plan* p, double alpha, double beta, cudaStream_t s) {
+  sht_ctx* ctx = p->ctx;
+  LaneLease lane(ctx);
+  const cudaStream_t ps = lane.lane.stream;
+  SHT_CUDA(cudaEventRecord(lane.lane.start, s));
+  split_layout(p, ctx->split_slices ? ctx->split_slices : split_slices_default(), s);
+  split_slice(p, alpha, s);
+  SHT_CUDA(cudaStreamWaitEvent(ps, lane.lane.start, 0));
+  plan_build(p, ps);
+  split_records(p, ps);
+  SHT_CUDA(cudaEventRecord(lane.lane.done, ps));
+  SHT_CUDA(cudaStreamWaitEvent(s, lane.lane.done, 0));
+  plan_touch(p, s);
+  split_launch(p, sparse_args(p, alpha, beta), s);
+  split_check(p, s);
+}
+
 static void prepare_mode(sht_plan* p, cudaStream_t s) {
   if (p->mode == SHT_MODE_BATCHED_FP64) batched_prepare(p, s);
   if (p->mode == SHT_MODE_SPLIT) split_prepare(p, p->ctx->split_slices ? p->ctx->split_slices : split_slices_default(), s);
@@ -62,6 +109,11 @@ sht_status sht_finalize(sht_ctx* ctx) {
     if (!ctx) return;
     cudaDeviceSynchronize();
     if (ctx->stage_stream) cudaStreamDestroy(ctx->stage_stream);
+    for (auto& l : ctx->lanes) {
+      cudaEventDestroy(l.start);
+      cudaEventDestroy(l.done);
+      cudaStreamDestroy(l.stream);
+    }
     delete ctx;
   });
 }
@@ -393,7 +445,8 @@ sht_status sht_plan_report(sht_plan* p, sht_contract_report* rep) {
     rep->nblocks_c = p->C->nblocks;
     rep->nnz_c = p->C->nnz;
     rep->nwork = p->mode == SHT_MODE_BATCHED_FP64 ? p->bwork : p->nwork;
-    rep->flops = p->flops;
+    if (p->flops_pending) SHT_CUDA(cudaDeviceSynchronize());  // the plan's stream is not known here
+    rep->flops = plan_flops(p, p->ctx->stage_stream);
     rep->plan_ms = p->plan_ms;
     rep->exec_ms = p->exec_ms;
     rep->slices = p->split_slices;
@@ -434,17 +487,22 @@ sht_status sht_contract(sht_ctx* ctx, const char* expr, double alpha, sht_tensor
     need(mode >= SHT_MODE_PLAIN_FP64 && mode <= SHT_MODE_SPLIT, "unknown mode");
     need(norm >= SHT_NORM_FROBENIUS && norm <= SHT_NORM_FROBENIUS_REFCOMPAT, "unknown norm");
     cudaStream_t s = as_stream(stream);
-    std::unique_ptr<sht_plan> p(plan_create(ctx, expr, A, B, C, eps, norm, mode, s));
-    prepare_mode(p.get(), s);
-    plan_execute(p.get(), alpha, beta, s);
-    if (p->mode == SHT_MODE_SPLIT) split_check(p.get(), s);
+    std::unique_ptr<sht_plan> p;
+    if (mode == SHT_MODE_SPLIT) {
+      p.reset(plan_init(ctx, expr, A, B, C, eps, norm, mode, s));
+      contract_split(p.get(), alpha, beta, s);
+    } else {
+      p.reset(plan_create(ctx, expr, A, B, C, eps, norm, mode, s));
+      prepare_mode(p.get(), s);
+      plan_execute(p.get(), alpha, beta, s);
+    }
     if (rep) {
       std::memset(rep, 0, sizeof(*rep));
       rep->npairs = p->npairs;
       rep->nblocks_c = C->nblocks;
       rep->nnz_c = C->nnz;
       rep->nwork = p->mode == SHT_MODE_BATCHED_FP64 ? p->bwork : p->nwork;
-      rep->flops = p->flops;
+      rep->flops = plan_flops(p.get(), s);
       rep->plan_ms = p->plan_ms;
       rep->slices = p->split_slices;
     }

@@ -238,6 +238,24 @@ static void launch_tiles(int cfg, long long nwork, const SparseArgs& g, cudaStre
   SHT_CUDA(cudaGetLastError());
 }
 
+// Count the product block ids (sorted, with repeats) that are absent from the stored C ids
+// (sorted, unique): zero means the result pattern is C's pattern.
+__global__ void k_count_missing(const long long* __restrict__ pc, long long np, const long long* __restrict__ cids,
+                                long long nc, unsigned long long* __restrict__ missing) {
+  unsigned long long n = 0;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < np; i += (long long)gridDim.x * blockDim.x) {
+    if (i > 0 && pc[i] == pc[i - 1]) continue;  // one search per distinct id
+    const long long id = pc[i];
+    long long lo = 0, hi = nc;
+    while (lo < hi) {
+      const long long mid = (lo + hi) >> 1;
+      if (cids[mid] < id) lo = mid + 1; else hi = mid;
+    }
+    if (lo == nc || cids[lo] != id) ++n;
+  }
+  if (n) atomicAdd(missing, n);
+}
+
 // ---------------------------------------------------------------------------------------
 // host side
 // ---------------------------------------------------------------------------------------
@@ -330,22 +348,39 @@ void cblock_stats(sht_plan* p, cudaStream_t s) {
   p->d_cn = PoolBuf(pool, std::max(nc, 1LL) * 4, s);
   p->d_cksum = PoolBuf(pool, std::max(nc, 1LL) * 8, s);
   p->flops = 0.0;
+  p->flops_pending = false;
   if (nc == 0) return;
-  PoolBuf fl(pool, nc * 8, s), tot(pool, 8, s);
+  PoolBuf fl(pool, nc * 8, s);
+  p->d_flops = PoolBuf(pool, 8, s);
   k_cstats<<<grid_for(nc, 256), 256, 0, s>>>(p->C->d_dims.as<int>(), p->C->order, p->tmaps.row, p->tmaps.col,
                                               p->d_pstart.as<int>(), p->d_pair_a.as<int>(), p->A->d_dims.as<int>(),
                                               p->A->order, p->tmaps.kk, nc, p->d_cm.as<int>(), p->d_cn.as<int>(),
                                               p->d_cksum.as<long long>(), fl.as<double>());
   SHT_CUDA(cudaGetLastError());
   size_t tb = 0;
-  cub::DeviceReduce::Sum(nullptr, tb, fl.as<double>(), tot.as<double>(), (int)nc, s);
+  cub::DeviceReduce::Sum(nullptr, tb, fl.as<double>(), p->d_flops.as<double>(), (int)nc, s);
   PoolBuf tmp(pool, tb, s);
-  cub::DeviceReduce::Sum(tmp.ptr, tb, fl.as<double>(), tot.as<double>(), (int)nc, s);
-  p->flops = d2h_scalar<double>(tot.ptr, s);
+  cub::DeviceReduce::Sum(tmp.ptr, tb, fl.as<double>(), p->d_flops.as<double>(), (int)nc, s);
+  p->flops_pending = true;  // read with the next synchronization (plan_flops)
+}
+
+double plan_flops(sht_plan* p, cudaStream_t s) {
+  if (p->flops_pending) {
+    p->flops = d2h_scalar<double>(p->d_flops.ptr, s);
+    p->flops_pending = false;
+  }
+  return p->flops;
 }
 
 sht_plan* plan_create(sht_ctx* ctx, const std::string& expr, sht_tensor* A, sht_tensor* B, sht_tensor* C,
                       double eps, sht_norm norm, sht_mode mode, cudaStream_t s) {
+  std::unique_ptr<sht_plan> p(plan_init(ctx, expr, A, B, C, eps, norm, mode, s));
+  plan_build(p.get(), s);
+  return p.release();
+}
+
+sht_plan* plan_init(sht_ctx* ctx, const std::string& expr, sht_tensor* A, sht_tensor* B, sht_tensor* C,
+                    double eps, sht_norm norm, sht_mode mode, cudaStream_t s) {
   const double t0 = now_ms();
   trace("plan: start", s);
   if (!A || !B || !C) fail(SHT_ERR_INVALID, "null tensor");
@@ -369,6 +404,22 @@ sht_plan* plan_create(sht_ctx* ctx, const std::string& expr, sht_tensor* A, sht_
   check_block_sizes(A, mp.rowA, C, mp.rowC, "tensor A", "tensor C");
   check_block_sizes(B, mp.colB, C, mp.colC, "tensor B", "tensor C");
   check_block_sizes(A, mp.colA, B, mp.rowB, "tensor A", "tensor B");
+  p->eps = eps;
+  p->norm = norm;
+  p->plan_ms = now_ms() - t0;
+  return p.release();
+}
+
+void plan_build(sht_plan* p, cudaStream_t s) {
+  const double t0 = now_ms();
+  sht_ctx* ctx = p->ctx;
+  sht_tensor *A = p->A, *B = p->B, *C = p->C;
+  // buffers the build reads or replaces are released against this stream
+  for (sht_tensor* t : {A, B, C}) tensor_touch(t, s);
+  const double eps = p->eps;
+  const sht_norm norm = p->norm;
+  const sht_mode mode = p->mode;
+  const ShtMaps& mp = p->maps;
   DevicePool* pool = ctx->pool.get();
   const long long nA = A->nblocks, nB = B->nblocks;
 
@@ -462,7 +513,17 @@ sht_plan* plan_create(sht_ctx* ctx, const std::string& expr, sht_tensor* A, sht_
   // result pattern: unique idC ∪ stored C ids
   long long nu = 0;
   PoolBuf uids;
-  if (np > 0) {
+  bool grow = np > 0;
+  if (np > 0 && C->nblocks > 0) {
+    // the repeated case: every product block is stored already (one count, no sorts)
+    PoolBuf miss(pool, 8, s);
+    SHT_CUDA(cudaMemsetAsync(miss.ptr, 0, 8, s));
+    k_count_missing<<<grid_for(np, 256), 256, 0, s>>>(pc_sorted.as<long long>(), np, C->d_ids.as<long long>(),
+                                                       C->nblocks, miss.as<unsigned long long>());
+    SHT_CUDA(cudaGetLastError());
+    grow = d2h_scalar<unsigned long long>(miss.ptr, s) > 0;
+  }
+  if (grow) {
     uids = PoolBuf(pool, np * 8, s);
     PoolBuf counts(pool, np * 4, s), nruns(pool, 8, s);
     size_t tb = 0;
@@ -550,15 +611,14 @@ sht_plan* plan_create(sht_ctx* ctx, const std::string& expr, sht_tensor* A, sht_
   p->tmaps.oB = B->order;
   p->tmaps.oC = C->order;
   // per C block m, n, sum of the pairs' k and flops; the total flop count
-  cblock_stats(p.get(), s);
+  cblock_stats(p, s);
   trace("plan: pstart+flops", s);
   if (mode == SHT_MODE_PLAIN_FP64) {
-    p->shape = choose_plain_shape(p.get());
-    build_work(p.get(), kShapes[p->shape].tm, kShapes[p->shape].tn, s);
+    p->shape = choose_plain_shape(p);
+    build_work(p, kShapes[p->shape].tm, kShapes[p->shape].tn, s);
     trace("plan: plain work list", s);
   }
-  p->plan_ms = now_ms() - t0;
-  return p.release();
+  p->plan_ms += now_ms() - t0;
 }
 
 void build_work(sht_plan* p, int TM, int TN, cudaStream_t s) {
@@ -584,6 +644,7 @@ void build_work(sht_plan* p, int TM, int TN, cudaStream_t s) {
   k_tile_emit<<<grid_for(nc, 128), 128, 0, s>>>(nc, ct.as<long long>(), ot.as<long long>(), cu.as<long long>(),
                                                  ou.as<long long>(), nt, p->d_work.as<int2>());
   SHT_CUDA(cudaGetLastError());
+  plan_flops(p, s);  // the stream is idle after the reads above
   p->nwork_touched = nt;
   p->nwork = nt + nu;
   p->work_tm = TM;

@@ -13,6 +13,10 @@ struct sht_plan {
   sht::TileMaps tmaps{};
   long long npairs = 0, ncblk = 0, nwork = 0, nwork_touched = 0;
   double flops = 0.0, plan_ms = 0.0, exec_ms = 0.0;
+  double eps = 0.0;                 // screening threshold and norm of the pair list
+  sht_norm norm = SHT_NORM_FROBENIUS;
+  sht::PoolBuf d_flops;             // device total of the flop count until it is read
+  bool flops_pending = false;       // d_flops not yet copied into flops
   int shape = 0, work_tm = 64, work_tn = 64;
   sht::PoolBuf d_pair_a, d_pair_b;  // int32 storage indices into A / B, canonical order
   sht::PoolBuf d_pstart;            // int32[ncblk + 1]
@@ -53,8 +57,16 @@ namespace sht {
 
 sht_plan* plan_create(sht_ctx* ctx, const std::string& expr, sht_tensor* A, sht_tensor* B, sht_tensor* C,
                       double eps, sht_norm norm, sht_mode mode, cudaStream_t s);
+// plan_create in two steps: the host checks and the parse (no device work but reading stale
+// host patterns back on s), then the pair list, result pattern and per-block statistics on s
+sht_plan* plan_init(sht_ctx* ctx, const std::string& expr, sht_tensor* A, sht_tensor* B, sht_tensor* C,
+                    double eps, sht_norm norm, sht_mode mode, cudaStream_t s);
+void plan_build(sht_plan* p, cudaStream_t s);
 void build_work(sht_plan* p, int TM, int TN, cudaStream_t s);
 void cblock_stats(sht_plan* p, cudaStream_t s);
+// The plan's flop count; the first call after planning copies it from the device (a sync),
+// so callers that synchronize anyway read it right after.
+double plan_flops(sht_plan* p, cudaStream_t s);
 // Cost-ordered work list (C block, tile, shape) on the device: fixed_shape >= 0 uses one
 // shape (tm x tn) for every block, otherwise per size class from class_shape (or the model).
 void device_work_list(sht_plan* p, int fixed_tm, int fixed_tn, bool per_class, cudaStream_t s);
@@ -69,8 +81,16 @@ long long batched_multi_launch(sht_ctx* ctx, const std::vector<sht_plan*>& plans
                                void* host_descs, PoolBuf& descs, PoolBuf& counter, int ctas_per_sm, cudaStream_t s);
 SparseArgs sparse_args(sht_plan* p, double alpha, double beta);
 void plan_touch(sht_plan* p, cudaStream_t s);  // plan buffers and tensors: next used on s
-void split_prepare(sht_plan* p, int S, cudaStream_t s);
-void split_execute(sht_plan* p, const SparseArgs& sa, cudaStream_t s);
+void split_prepare(sht_plan* p, int S, cudaStream_t s);  // split_layout + split_records
+void split_execute(sht_plan* p, const SparseArgs& sa, cudaStream_t s);  // split_slice + split_launch
+// slice buffers and the slicer's items: depends on the patterns of A and B only
+void split_layout(sht_plan* p, int S, cudaStream_t s);
+// work list, C offset tables, tile and pair records: needs plan_build
+void split_records(sht_plan* p, cudaStream_t s);
+// the slicer over A (scaled by alpha) and B: needs split_layout only
+void split_slice(sht_plan* p, double alpha, cudaStream_t s);
+// the tensor-core kernel: needs everything above
+void split_launch(sht_plan* p, const SparseArgs& sa, cudaStream_t s);
 void split_check(sht_plan* p, cudaStream_t s);
 int split_slices_default();
 void matform_execute(sht_plan* p, double alpha, cudaStream_t s);

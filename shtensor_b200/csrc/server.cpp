@@ -355,7 +355,7 @@ void sht_server::planner(int index) {
       if (!g.sc.alpha_zero) sht::matform_execute(r->plan.get(), r->alpha, s);
       SHT_CUDA(cudaEventRecord(r->planned, s));
       r->npairs = r->plan->npairs;
-      r->flops = r->plan->flops;
+      r->flops = sht::plan_flops(r->plan.get(), s);
     } catch (const sht::Error& e) {
       r->plan.reset();
       cudaStreamSynchronize(s);

@@ -157,6 +157,14 @@ struct sht_ctx {
   // handle made from the context is destroyed
   std::shared_ptr<sht::DevicePool> pool;
   cudaStream_t stage_stream = nullptr;  // host-staging copies
+  // non-blocking streams, each with two events, lent to contractions that plan on a second
+  // stream while the caller's stream slices the operands (created on demand, kept)
+  struct Lane {
+    cudaStream_t stream = nullptr;
+    cudaEvent_t start = nullptr, done = nullptr;
+  };
+  std::mutex lanes_mu;
+  std::vector<Lane> lanes;
   std::map<std::string, int> tuned;     // autotuner choices: size-class key -> tile id
   int split_slices = 0;                 // INT8 slices per operand in split mode (0 = default)
 };

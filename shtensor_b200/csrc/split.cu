@@ -683,6 +683,11 @@ static void slice_layout(const sht_tensor* T, const std::vector<int>& free_modes
 int split_slices_default() { return 7; }
 
 void split_prepare(sht_plan* p, int S, cudaStream_t s) {
+  split_layout(p, S, s);
+  split_records(p, s);
+}
+
+void split_layout(sht_plan* p, int S, cudaStream_t s) {
   if (S < 1 || S > kMaxSlices) fail(SHT_ERR_INVALID, "split slices must be 1..8");
   DevicePool* pool = p->ctx->pool.get();
   p->split_slices = S;
@@ -717,9 +722,13 @@ void split_prepare(sht_plan* p, int S, cudaStream_t s) {
     SHT_CUDA(cudaMemcpyAsync(p->sp_boff.ptr, bo.data(), nB * 8, cudaMemcpyHostToDevice, s));
     SHT_CUDA(cudaMemcpyAsync(p->sp_beoff.ptr, be.data(), nB * 8, cudaMemcpyHostToDevice, s));
   }
+  // (copies from pageable memory have consumed their source when they return)
   SHT_CUDA(cudaMemsetAsync(p->sp_err.ptr, 0, 256, s));
-  SHT_CUDA(cudaStreamSynchronize(s));
   trace("split: slice layout", s);
+}
+
+void split_records(sht_plan* p, cudaStream_t s) {
+  DevicePool* pool = p->ctx->pool.get();
   // work list: 128 x 32 tiles of every C block, heaviest blocks first, with per-tile and
   // per-pair records so that the kernel reads each with one load
   device_work_list(p, kSplitM, kSplitN, false, s);
@@ -774,7 +783,6 @@ void split_prepare(sht_plan* p, int S, cudaStream_t s) {
         p->sp_boff.as<long long>(), p->sp_aeoff.as<long long>(), p->sp_beoff.as<long long>(),
         p->A->d_dims.as<int>(), p->tmaps, p->sp_pairs.as<SplitPair>());
   SHT_CUDA(cudaGetLastError());
-  SHT_CUDA(cudaStreamSynchronize(s));
   trace("split: tile / pair records", s);
 }
 
@@ -800,14 +808,21 @@ static int split_grid(sht_ctx* ctx) {
 }
 
 void split_execute(sht_plan* p, const SparseArgs& sa, cudaStream_t s) {
+  split_slice(p, sa.sc.alpha, s);
+  split_launch(p, sa, s);
+}
+
+void split_slice(sht_plan* p, double alpha, cudaStream_t s) {
   const int S = p->split_slices;
-  if (!sa.sc.alpha_zero) {
+  uint64_t ab;
+  std::memcpy(&ab, &alpha, 8);
+  if (ab != 0) {
     const long long cap = (long long)p->ctx->num_sms * 16;
     if (p->sp_naitems)
       k_slice<<<(int)std::min((p->sp_naitems + 7) / 8, cap), 256, 0, s>>>(
           p->A->d_data.as<double>(), p->A->d_offsets.as<long long>(), p->A->d_dims.as<int>(), p->A->order,
           modes_of(p->maps.rowA), modes_of(p->maps.colA), p->sp_aoff.as<long long>(), p->sp_aeoff.as<long long>(),
-          p->sp_a.as<signed char>(), p->sp_ae.as<short>(), sa.sc.alpha, S, kSplitM, p->sp_aitems.as<int2>(),
+          p->sp_a.as<signed char>(), p->sp_ae.as<short>(), alpha, S, kSplitM, p->sp_aitems.as<int2>(),
           p->sp_naitems, p->sp_err.as<int>() + 1);
     if (p->sp_nbitems)
       k_slice<<<(int)std::min((p->sp_nbitems + 7) / 8, cap), 256, 0, s>>>(
@@ -817,6 +832,10 @@ void split_execute(sht_plan* p, const SparseArgs& sa, cudaStream_t s) {
           p->sp_err.as<int>() + 1);
     SHT_CUDA(cudaGetLastError());
   }
+}
+
+void split_launch(sht_plan* p, const SparseArgs& sa, cudaStream_t s) {
+  const int S = p->split_slices;
   uint64_t one, bb;
   const double d1 = 1.0;
   std::memcpy(&one, &d1, 8);

@@ -97,3 +97,50 @@ def test_compare_entry_point(ctx):
     sht.contract(ctx, w.expr, 1.0, A, B, 0.0, C2, mode=sht.Mode.SPLIT)
     mx, fro = sht.compare(C2, C1)
     assert 0.0 <= fro <= REL_TOL and mx >= 0.0
+
+
+def per_block_errors(ctx, w):
+    """Run the split form and return, per C block, (relative error, max abs error, max |want|)."""
+    A, B, C = dev(ctx, w.A), dev(ctx, w.B), dev(ctx, w.C)
+    sht.contract(ctx, w.expr, 1.0, A, B, 0.0, C, mode=sht.Mode.SPLIT)
+    want = oracle.contract(w.expr, 1.0, host(w.A), host(w.B), 0.0, host(w.C))
+    ids, offs, _ = C.get_sparse_info()
+    assert np.array_equal(ids, want.C.ids)
+    got = C.download()
+    ends = np.append(offs[1:], got.size)
+    out = []
+    for o, e in zip(offs, ends):
+        g, r = got[o:e], want.C.data[o:e]
+        scale = np.abs(r).max()
+        # relative to the block's largest value (no squares: values reach 1e300)
+        out.append((float(np.abs(g - r).max() / scale) if scale > 0 else 0.0, float(np.abs(g - r).max()), scale))
+    return out
+
+
+def test_split_extreme_exponents(ctx):
+    # row / column exponents far outside [-480, 480] and subnormal products take the general
+    # conversion and scaling; in-range ones the scale-folded conversion; same launch
+    rng = np.random.default_rng(11)
+    bi, bk, bj = [8, 12, 16], [20, 40], [10, 24, 6]
+    sa, sb = np.array([1e-150, 1.0, 1e150]), np.array([1e150, 1e-160, 1.0])
+    A = W.build_tensor(rng, [bi, bk], lambda c: np.ones(len(c[0]), bool), lambda c: sa[c[0]], "normal")
+    B = W.build_tensor(rng, [bk, bj], lambda c: np.ones(len(c[0]), bool), lambda c: sb[c[1]], "normal")
+    w = W.Workload("extreme", "ik, kj -> ij", A, B, W.empty_tensor([bi, bj]))
+    for rel, mx, scale in per_block_errors(ctx, w):
+        if scale < 1e-300:
+            # subnormal results: the oracle rounds every product to the subnormal grid
+            assert mx <= 64 * 5e-324 * 60, (mx, scale)
+        else:
+            assert rel <= 1e-13, (rel, scale)
+
+
+def test_split_long_contracted_extent(ctx):
+    # K = 9728: seven INT32 groups of up to 7 * 127^2 * K no longer fit the scale-folded
+    # conversion of the low part (|L| >= 2^51 possible), so the launch converts generally
+    rng = np.random.default_rng(12)
+    bi, bk, bj = [8, 24], [9728], [16, 8]
+    A = W.build_tensor(rng, [bi, bk], lambda c: np.ones(len(c[0]), bool), None, "normal")
+    B = W.build_tensor(rng, [bk, bj], lambda c: np.ones(len(c[0]), bool), None, "normal")
+    w = W.Workload("long_k", "ik, kj -> ij", A, B, W.empty_tensor([bi, bj]))
+    errs = per_block_errors(ctx, w)
+    assert max(e[0] for e in errs) <= REL_TOL, errs
