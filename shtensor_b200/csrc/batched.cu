@@ -297,7 +297,10 @@ __global__ void k_block_shapes(const int* __restrict__ cm, const int* __restrict
     shape[c] = sh;
     tiles[c] = nt;
     touched_tiles[c] = np > 0 ? nt : 0;
-    key[c] = np > 0 ? (unsigned long long)(tm * tn) * (unsigned long long)ks + 1ull : 0ull;
+    // cost of one tile, coarsened to 16 bits (the float's exponent and 7 mantissa bits: the
+    // order is for load balance only, and the stable sort keeps ties in block order)
+    const float cost = np > 0 ? (float)((double)(tm * tn) * (double)ks + 1.0) : 0.0f;
+    key[c] = (unsigned long long)(__float_as_uint(cost) >> 16);
     idx[c] = (int)c;
   }
 }
@@ -351,12 +354,12 @@ void device_work_list(sht_plan* p, int fixed_tm, int fixed_tn, bool per_class, c
   SHT_CUDA(cudaGetLastError());
   size_t tb = 0, tb2 = 0, tb3 = 0;
   cub::DeviceRadixSort::SortPairsDescending(nullptr, tb, key.as<unsigned long long>(), key2.as<unsigned long long>(),
-                                            idx.as<int>(), idx2.as<int>(), (int)nc, 0, 64, s);
+                                            idx.as<int>(), idx2.as<int>(), (int)nc, 0, 16, s);
   cub::DeviceScan::ExclusiveSum(nullptr, tb2, tsorted.as<long long>(), off.as<long long>(), (int)nc, s);
   cub::DeviceReduce::Sum(nullptr, tb3, ttiles.as<long long>(), sums.as<long long>(), (int)nc, s);
   PoolBuf tmp(pool, std::max(tb, std::max(tb2, tb3)), s);
   cub::DeviceRadixSort::SortPairsDescending(tmp.ptr, tb, key.as<unsigned long long>(), key2.as<unsigned long long>(),
-                                            idx.as<int>(), idx2.as<int>(), (int)nc, 0, 64, s);
+                                            idx.as<int>(), idx2.as<int>(), (int)nc, 0, 16, s);
   k_gather_tiles<<<grid_for(nc, 256), 256, 0, s>>>(idx2.as<int>(), tiles.as<long long>(), nc, tsorted.as<long long>());
   cub::DeviceScan::ExclusiveSum(tmp.ptr, tb2, tsorted.as<long long>(), off.as<long long>(), (int)nc, s);
   cub::DeviceReduce::Sum(tmp.ptr, tb3, ttiles.as<long long>(), sums.as<long long>(), (int)nc, s);

@@ -25,7 +25,11 @@ struct LaneLease {
         return;
       }
     }
-    SHT_CUDA(cudaStreamCreateWithFlags(&lane.stream, cudaStreamNonBlocking));
+    // the highest priority: the plan's short kernels are scheduled ahead of the slicer's
+    // remaining blocks on the caller's stream
+    int lo = 0, hi = 0;
+    SHT_CUDA(cudaDeviceGetStreamPriorityRange(&lo, &hi));
+    SHT_CUDA(cudaStreamCreateWithPriority(&lane.stream, cudaStreamNonBlocking, hi));
     SHT_CUDA(cudaEventCreateWithFlags(&lane.start, cudaEventDisableTiming));
     SHT_CUDA(cudaEventCreateWithFlags(&lane.done, cudaEventDisableTiming));
   }
@@ -49,6 +53,7 @@ static void contract_split(sht_plan* p, double alpha, double beta, cudaStream_t 
   SHT_CUDA(cudaEventRecord(lane.lane.start, s));
   split_layout(p, ctx->split_slices ? ctx->split_slices : split_slices_default(), s);
   split_slice(p, alpha, s);
+  trace("contract: slicer launched", s);
   SHT_CUDA(cudaStreamWaitEvent(ps, lane.lane.start, 0));
   plan_build(p, ps);
   split_records(p, ps);
@@ -56,7 +61,9 @@ static void contract_split(sht_plan* p, double alpha, double beta, cudaStream_t 
   SHT_CUDA(cudaStreamWaitEvent(s, lane.lane.done, 0));
   plan_touch(p, s);
   split_launch(p, sparse_args(p, alpha, beta), s);
+  trace("contract: split kernel launched", s);
   split_check(p, s);
+  trace("contract: checked", s);
 }
 
 static void prepare_mode(sht_plan* p, cudaStream_t s) {

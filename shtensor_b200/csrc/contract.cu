@@ -31,13 +31,15 @@ double now_ms() {
 }
 
 void trace(const char* what, cudaStream_t s) {
-  static const bool on = [] {
+  // SHT_TRACE=1: synchronize at every point (device + host time per phase);
+  // SHT_TRACE=2: host time only (what the host spends issuing each phase)
+  static const int on = [] {
     const char* e = std::getenv("SHT_TRACE");
-    return e && e[0] == '1';
+    return e && (e[0] == '1' || e[0] == '2') ? e[0] - '0' : 0;
   }();
   if (!on) return;
   static double last = 0;
-  cudaStreamSynchronize(s);
+  if (on == 1) cudaStreamSynchronize(s);
   const double t = now_ms();
   std::fprintf(stderr, "[sht] %-28s %8.3f ms\n", what, last > 0 ? t - last : 0.0);
   last = t;
@@ -115,11 +117,11 @@ __global__ void k_emit(const unsigned long long* __restrict__ keyA, const long l
                        const unsigned long long* __restrict__ keyBs, const int* __restrict__ permB,
                        const long long* __restrict__ partB, long long nB, const double* __restrict__ normA,
                        const double* __restrict__ normB, double eps, const long long* __restrict__ lo_in,
-                       const long long* __restrict__ off, long long* __restrict__ pc, int* __restrict__ pa,
-                       int* __restrict__ pb) {
+                       const long long* __restrict__ end, const long long* __restrict__ cnt, long long* __restrict__ pc,
+                       int* __restrict__ pa, int* __restrict__ pb) {
   for (long long a = blockIdx.x * (long long)blockDim.x + threadIdx.x; a < nA; a += (long long)gridDim.x * blockDim.x) {
     const unsigned long long k = keyA[a];
-    long long w = off[a];
+    long long w = end[a] - cnt[a];  // inclusive prefix sum minus own count
     const long long pA = partA[a];
     const double na = normA ? normA[a] : 0.0;
     for (long long j = lo_in[a]; j < nB && keyBs[j] == k; ++j) {
@@ -452,13 +454,23 @@ void plan_build(sht_plan* p, cudaStream_t s) {
     k_keys<<<grid_for(nB, 256), 256, 0, s>>>(make_meta(B), kb, B->d_ids.as<long long>(), nB,
                                               keyB.as<unsigned long long>(), partB.as<long long>());
     SHT_CUDA(cudaGetLastError());
-    PoolBuf keyBs(pool, nB * 8, s), iota(pool, nB * 4, s), permB(pool, nB * 4, s);
+    PoolBuf keyBs, iota(pool, nB * 4, s), permB;
     k_iota<<<grid_for(nB, 256), 256, 0, s>>>(iota.as<int>(), nB);
+    // B's blocks are stored by id (column-major over the block grid): when the contracted
+    // modes are B's last modes, in order, the keys already ascend in storage order
+    bool b_sorted = true;
+    for (size_t t = 0; t < mp.rowB.size(); ++t)
+      b_sorted = b_sorted && mp.rowB[t] == B->order - (int)mp.rowB.size() + (int)t;
     const int kbits = bits_for(kspan);
     size_t tb = 0;
-    cub::DeviceRadixSort::SortPairs(nullptr, tb, keyB.as<unsigned long long>(), keyBs.as<unsigned long long>(),
-                                    iota.as<int>(), permB.as<int>(), (int)nB, 0, kbits, s);
-    {
+    if (b_sorted) {
+      keyBs = std::move(keyB);
+      permB = std::move(iota);
+    } else {
+      keyBs = PoolBuf(pool, nB * 8, s);
+      permB = PoolBuf(pool, nB * 4, s);
+      cub::DeviceRadixSort::SortPairs(nullptr, tb, keyB.as<unsigned long long>(), keyBs.as<unsigned long long>(),
+                                      iota.as<int>(), permB.as<int>(), (int)nB, 0, kbits, s);
       PoolBuf tmp(pool, tb, s);
       cub::DeviceRadixSort::SortPairs(tmp.ptr, tb, keyB.as<unsigned long long>(), keyBs.as<unsigned long long>(),
                                       iota.as<int>(), permB.as<int>(), (int)nB, 0, kbits, s);
@@ -475,19 +487,20 @@ void plan_build(sht_plan* p, cudaStream_t s) {
                                               permB.as<int>(), nB, normA.as<double>(), normB.as<double>(), eps,
                                               lo.as<long long>(), cnt.as<long long>());
     SHT_CUDA(cudaGetLastError());
-    cub::DeviceScan::ExclusiveSum(nullptr, tb, cnt.as<long long>(), off.as<long long>(), (int)nA, s);
+    cub::DeviceScan::InclusiveSum(nullptr, tb, cnt.as<long long>(), off.as<long long>(), (int)nA, s);
     {
       PoolBuf tmp(pool, tb, s);
-      cub::DeviceScan::ExclusiveSum(tmp.ptr, tb, cnt.as<long long>(), off.as<long long>(), (int)nA, s);
+      cub::DeviceScan::InclusiveSum(tmp.ptr, tb, cnt.as<long long>(), off.as<long long>(), (int)nA, s);
     }
-    np = d2h_scalar<long long>(off.as<long long>() + nA - 1, s) + d2h_scalar<long long>(cnt.as<long long>() + nA - 1, s);
+    np = d2h_scalar<long long>(off.as<long long>() + nA - 1, s);
     if (np > (long long)INT32_MAX) fail(SHT_ERR_UNSUPPORTED, "more than 2^31 block pairs");
     if (np > 0) {
       PoolBuf pc(pool, np * 8, s), pa(pool, np * 4, s), pb(pool, np * 4, s);
       k_emit<<<grid_for(nA, 128), 128, 0, s>>>(keyA.as<unsigned long long>(), partA.as<long long>(), nA,
                                                keyBs.as<unsigned long long>(), permB.as<int>(), partB.as<long long>(),
                                                nB, normA.as<double>(), normB.as<double>(), eps, lo.as<long long>(),
-                                               off.as<long long>(), pc.as<long long>(), pa.as<int>(), pb.as<int>());
+                                               off.as<long long>(), cnt.as<long long>(), pc.as<long long>(),
+                                               pa.as<int>(), pb.as<int>());
       SHT_CUDA(cudaGetLastError());
       PoolBuf pidx(pool, np * 4, s), porder(pool, np * 4, s);
       pc_sorted = PoolBuf(pool, np * 8, s);
@@ -673,8 +686,7 @@ void plan_touch(sht_plan* p, cudaStream_t s) {
                      &p->mf_b, &p->mf_aoff, &p->mf_boff, &p->mf_ald, &p->mf_bld, &p->mf_ak4, &p->mf_aitems,
                      &p->mf_bitems})
     b->use_on(s);
-  for (PoolBuf* b : {&p->sp_a, &p->sp_b, &p->sp_ae, &p->sp_be, &p->sp_aoff, &p->sp_boff, &p->sp_aeoff, &p->sp_beoff,
-                     &p->sp_err, &p->sp_aitems, &p->sp_bitems, &p->sp_items, &p->sp_pairs,
+  for (PoolBuf* b : {&p->sp_a, &p->sp_b, &p->sp_ae, &p->sp_be, &p->sp_meta, &p->sp_items, &p->sp_pairs,
                      &p->sp_rowtab, &p->sp_coltab})
     b->use_on(s);
 }

@@ -37,8 +37,13 @@ struct sht_plan {
   long long mf_naitems = 0, mf_nbitems = 0;
   long long mf_elems = 0;
   // split path: INT8 slices (K-major rows), row / column exponents, error words
-  sht::PoolBuf sp_a, sp_b, sp_ae, sp_be, sp_aoff, sp_boff, sp_aeoff, sp_beoff, sp_err;
-  sht::PoolBuf sp_aitems, sp_bitems;  // int2 (block, first row) items of 32 rows for the slicer
+  sht::PoolBuf sp_a, sp_b, sp_ae, sp_be;
+  // one upload: per-block slice and exponent offsets of A and B, the slicer's int2 (block,
+  // first row) items of 32 rows, and the kernels' error words (zero)
+  sht::PoolBuf sp_meta;
+  long long *sp_aoff = nullptr, *sp_aeoff = nullptr, *sp_boff = nullptr, *sp_beoff = nullptr;
+  int2 *sp_aitems = nullptr, *sp_bitems = nullptr;
+  int* sp_err = nullptr;
   long long sp_naitems = 0, sp_nbitems = 0;
   sht::PoolBuf sp_items, sp_pairs;    // per-tile and per-pair records of the split kernel
   sht::PoolBuf sp_rowtab, sp_coltab;  // element offsets of every C row / column in its block

@@ -196,6 +196,10 @@ struct sht_tensor {
   // host index (authoritative unless host_stale)
   std::vector<int64_t> ids, offsets, rows;
   bool host_stale = false;
+  // per-block extents (nblocks x order) of the host index, computed on first use after the
+  // host index changes (tensor_host_dims)
+  std::vector<int> hdims;
+  bool hdims_valid = false;
   int64_t nblocks = 0, nnz = 0;
   // device arrays
   sht::PoolBuf d_bsizes;   // int32, concatenated per mode
@@ -216,6 +220,8 @@ void parse_einsum(const std::string& expr, int nA, const int* sA, int nB, const 
 // tensors (tensor.cu)
 void tensor_set_index(sht_tensor* t, std::vector<int64_t>&& ids, cudaStream_t s);
 void tensor_sync_host(sht_tensor* t, cudaStream_t s);
+// per-block extents of the host index, nblocks x order (the host index must be current)
+const int* tensor_host_dims(sht_tensor* t);
 void tensor_upload_index(sht_tensor* t, cudaStream_t s);
 void tensor_norms_device(sht_tensor* t, sht_norm norm, double* d_out, cudaStream_t s);
 // Record that `s` uses the tensor's device buffers: when they are freed, reuse of the memory

@@ -656,18 +656,17 @@ static ModeMap modes_of(const std::vector<int>& v) {
 // Per block: byte offset of its slices (tiles of R rows) and offset of its exponents (rows
 // padded to a multiple of R), plus the slicer's items of 32 rows.  Groups hold exact INT32
 // sums of up to S products of |s| <= 127 per k, so K is limited to keep them below 2^31.
-static void slice_layout(const sht_tensor* T, const std::vector<int>& free_modes, const std::vector<int>& k_modes,
-                         int S, int R, std::vector<long long>& off, std::vector<long long>& eoff, long long& total,
-                         long long& etotal, std::vector<int2>& items) {
+static void slice_layout(sht_tensor* T, const std::vector<int>& free_modes, const std::vector<int>& k_modes,
+                         int S, int R, long long* off, long long* eoff, long long& total, long long& etotal,
+                         std::vector<int2>& items) {
   const long long n = T->nblocks;
-  off.resize(n);
-  eoff.resize(n);
+  const int* dims = tensor_host_dims(T);
   total = etotal = 0;
   for (long long b = 0; b < n; ++b) {
-    const int64_t id = T->ids[b];
+    const int* d = dims + b * T->order;
     long long m = 1, K = 1;
-    for (int ax : free_modes) m *= T->bs[ax][(id / T->gstride[ax]) % T->nblk[ax]];
-    for (int ax : k_modes) K *= T->bs[ax][(id / T->gstride[ax]) % T->nblk[ax]];
+    for (int ax : free_modes) m *= d[ax];
+    for (int ax : k_modes) K *= d[ax];
     if (K > 16384) fail(SHT_ERR_UNSUPPORTED, "split mode: contracted block extent above 16384");
     const long long Kp = (K + kSplitK - 1) / kSplitK * kSplitK;
     const long long mp = (m + R - 1) / R * R;
@@ -691,39 +690,36 @@ void split_layout(sht_plan* p, int S, cudaStream_t s) {
   if (S < 1 || S > kMaxSlices) fail(SHT_ERR_INVALID, "split slices must be 1..8");
   DevicePool* pool = p->ctx->pool.get();
   p->split_slices = S;
-  std::vector<long long> ao, ae, bo, be;
+  const long long nA = p->A->nblocks, nB = p->B->nblocks;
+  // host image of sp_meta: [A offsets | A exponent offsets | B offsets | B exponent offsets |
+  // error words (32 x 8 bytes) | A items | B items], 8-byte words
+  std::vector<long long> meta((size_t)(2 * nA + 2 * nB + 32));
   std::vector<int2> ia, ib;
   long long at, aet, bt, bet;
-  slice_layout(p->A, p->maps.rowA, p->maps.colA, S, kSplitM, ao, ae, at, aet, ia);
-  slice_layout(p->B, p->maps.colB, p->maps.rowB, S, kSplitN, bo, be, bt, bet, ib);
-  const long long nA = p->A->nblocks, nB = p->B->nblocks;
+  slice_layout(p->A, p->maps.rowA, p->maps.colA, S, kSplitM, meta.data(), meta.data() + nA, at, aet, ia);
+  slice_layout(p->B, p->maps.colB, p->maps.rowB, S, kSplitN, meta.data() + 2 * nA, meta.data() + 2 * nA + nB, bt,
+               bet, ib);
+  const size_t head = meta.size();
+  meta.resize(head + ia.size() + ib.size());
+  std::memcpy(meta.data() + head, ia.data(), ia.size() * sizeof(int2));
+  std::memcpy(meta.data() + head + ia.size(), ib.data(), ib.size() * sizeof(int2));
   p->sp_a = PoolBuf(pool, std::max(at, 16LL), s);
   p->sp_b = PoolBuf(pool, std::max(bt, 16LL), s);
   p->sp_ae = PoolBuf(pool, std::max(aet, 1LL) * 2, s);
   p->sp_be = PoolBuf(pool, std::max(bet, 1LL) * 2, s);
-  p->sp_aoff = PoolBuf(pool, std::max(nA, 1LL) * 8, s);
-  p->sp_aeoff = PoolBuf(pool, std::max(nA, 1LL) * 8, s);
-  p->sp_boff = PoolBuf(pool, std::max(nB, 1LL) * 8, s);
-  p->sp_beoff = PoolBuf(pool, std::max(nB, 1LL) * 8, s);
-  p->sp_err = PoolBuf(pool, 256, s);
-  p->sp_aitems = PoolBuf(pool, std::max<size_t>(ia.size(), 1) * sizeof(int2), s);
-  p->sp_bitems = PoolBuf(pool, std::max<size_t>(ib.size(), 1) * sizeof(int2), s);
+  p->sp_meta = PoolBuf(pool, meta.size() * 8, s);
+  long long* dm = p->sp_meta.as<long long>();
+  p->sp_aoff = dm;
+  p->sp_aeoff = dm + nA;
+  p->sp_boff = dm + 2 * nA;
+  p->sp_beoff = dm + 2 * nA + nB;
+  p->sp_err = reinterpret_cast<int*>(dm + 2 * nA + 2 * nB);
+  p->sp_aitems = reinterpret_cast<int2*>(dm + head);
+  p->sp_bitems = reinterpret_cast<int2*>(dm + head + ia.size());
   p->sp_naitems = (long long)ia.size();
   p->sp_nbitems = (long long)ib.size();
-  if (!ia.empty())
-    SHT_CUDA(cudaMemcpyAsync(p->sp_aitems.ptr, ia.data(), ia.size() * sizeof(int2), cudaMemcpyHostToDevice, s));
-  if (!ib.empty())
-    SHT_CUDA(cudaMemcpyAsync(p->sp_bitems.ptr, ib.data(), ib.size() * sizeof(int2), cudaMemcpyHostToDevice, s));
-  if (nA) {
-    SHT_CUDA(cudaMemcpyAsync(p->sp_aoff.ptr, ao.data(), nA * 8, cudaMemcpyHostToDevice, s));
-    SHT_CUDA(cudaMemcpyAsync(p->sp_aeoff.ptr, ae.data(), nA * 8, cudaMemcpyHostToDevice, s));
-  }
-  if (nB) {
-    SHT_CUDA(cudaMemcpyAsync(p->sp_boff.ptr, bo.data(), nB * 8, cudaMemcpyHostToDevice, s));
-    SHT_CUDA(cudaMemcpyAsync(p->sp_beoff.ptr, be.data(), nB * 8, cudaMemcpyHostToDevice, s));
-  }
-  // (copies from pageable memory have consumed their source when they return)
-  SHT_CUDA(cudaMemsetAsync(p->sp_err.ptr, 0, 256, s));
+  // one copy (from pageable memory it has consumed its source when it returns)
+  SHT_CUDA(cudaMemcpyAsync(dm, meta.data(), meta.size() * 8, cudaMemcpyHostToDevice, s));
   trace("split: slice layout", s);
 }
 
@@ -779,8 +775,8 @@ void split_records(sht_plan* p, cudaStream_t s) {
                                                           p->sp_items.as<SplitItem>());
   if (p->npairs > 0)
     k_split_pairs<<<grid_for(p->npairs, 256), 256, 0, s>>>(
-        p->d_pair_a.as<int>(), p->d_pair_b.as<int>(), p->npairs, p->sp_aoff.as<long long>(),
-        p->sp_boff.as<long long>(), p->sp_aeoff.as<long long>(), p->sp_beoff.as<long long>(),
+        p->d_pair_a.as<int>(), p->d_pair_b.as<int>(), p->npairs, p->sp_aoff,
+        p->sp_boff, p->sp_aeoff, p->sp_beoff,
         p->A->d_dims.as<int>(), p->tmaps, p->sp_pairs.as<SplitPair>());
   SHT_CUDA(cudaGetLastError());
   trace("split: tile / pair records", s);
@@ -821,15 +817,15 @@ void split_slice(sht_plan* p, double alpha, cudaStream_t s) {
     if (p->sp_naitems)
       k_slice<<<(int)std::min((p->sp_naitems + 7) / 8, cap), 256, 0, s>>>(
           p->A->d_data.as<double>(), p->A->d_offsets.as<long long>(), p->A->d_dims.as<int>(), p->A->order,
-          modes_of(p->maps.rowA), modes_of(p->maps.colA), p->sp_aoff.as<long long>(), p->sp_aeoff.as<long long>(),
-          p->sp_a.as<signed char>(), p->sp_ae.as<short>(), alpha, S, kSplitM, p->sp_aitems.as<int2>(),
-          p->sp_naitems, p->sp_err.as<int>() + 1);
+          modes_of(p->maps.rowA), modes_of(p->maps.colA), p->sp_aoff, p->sp_aeoff,
+          p->sp_a.as<signed char>(), p->sp_ae.as<short>(), alpha, S, kSplitM, p->sp_aitems,
+          p->sp_naitems, p->sp_err + 1);
     if (p->sp_nbitems)
       k_slice<<<(int)std::min((p->sp_nbitems + 7) / 8, cap), 256, 0, s>>>(
           p->B->d_data.as<double>(), p->B->d_offsets.as<long long>(), p->B->d_dims.as<int>(), p->B->order,
-          modes_of(p->maps.colB), modes_of(p->maps.rowB), p->sp_boff.as<long long>(), p->sp_beoff.as<long long>(),
-          p->sp_b.as<signed char>(), p->sp_be.as<short>(), 1.0, S, kSplitN, p->sp_bitems.as<int2>(), p->sp_nbitems,
-          p->sp_err.as<int>() + 1);
+          modes_of(p->maps.colB), modes_of(p->maps.rowB), p->sp_boff, p->sp_beoff,
+          p->sp_b.as<signed char>(), p->sp_be.as<short>(), 1.0, S, kSplitN, p->sp_bitems, p->sp_nbitems,
+          p->sp_err + 1);
     SHT_CUDA(cudaGetLastError());
   }
 }
@@ -855,7 +851,7 @@ void split_launch(sht_plan* p, const SparseArgs& sa, cudaStream_t s) {
   g.items = p->sp_items.as<SplitItem>();
   g.prs = p->sp_pairs.as<SplitPair>();
   g.nwork = (int)((bb == one) ? p->bwork_touched : p->bwork);
-  g.err = p->sp_err.as<int>();
+  g.err = p->sp_err;
   g.wait_limit = 1LL << 22;
   if (g.nwork <= 0) return;
   const int grid = (int)std::min<long long>(split_grid(p->ctx), g.nwork);
@@ -932,7 +928,7 @@ double measure_int8_tops(sht_ctx* ctx) {
 // error words of the last split execute: [0] status from bounded waits, [1] non-finite input
 void split_check(sht_plan* p, cudaStream_t s) {
   int e[2] = {0, 0};
-  SHT_CUDA(cudaMemcpyAsync(e, p->sp_err.ptr, 8, cudaMemcpyDeviceToHost, s));
+  SHT_CUDA(cudaMemcpyAsync(e, p->sp_err, 8, cudaMemcpyDeviceToHost, s));
   SHT_CUDA(cudaStreamSynchronize(s));
   if (e[0]) fail((sht_status)e[0], "split-precision kernel: a bounded wait on the tensor cores expired");
   if (e[1]) fail(SHT_ERR_UNSUPPORTED, "split-precision mode needs finite inputs");

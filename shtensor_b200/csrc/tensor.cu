@@ -65,6 +65,7 @@ void block_dims_sizes(const sht_tensor* t, const long long* ids, long long n, in
 void tensor_set_index(sht_tensor* t, std::vector<int64_t>&& ids, cudaStream_t s) {
   DevicePool* pool = t->ctx->pool.get();
   t->ids = std::move(ids);
+  t->hdims_valid = false;
   t->nblocks = static_cast<int64_t>(t->ids.size());
   t->offsets.resize(t->ids.size());
   int64_t off = 0;
@@ -94,6 +95,18 @@ void tensor_set_index(sht_tensor* t, std::vector<int64_t>&& ids, cudaStream_t s)
   SHT_CUDA(cudaStreamSynchronize(s));
 }
 
+const int* tensor_host_dims(sht_tensor* t) {
+  if (!t->hdims_valid) {
+    t->hdims.resize(std::max<size_t>(t->ids.size() * t->order, 1));
+    for (size_t b = 0; b < t->ids.size(); ++b) {
+      const int64_t id = t->ids[b] >= 0 ? t->ids[b] : -(t->ids[b] + 1);  // marked ids are -(id)-1
+      for (int d = 0; d < t->order; ++d) t->hdims[b * t->order + d] = t->bs[d][(id / t->gstride[d]) % t->nblk[d]];
+    }
+    t->hdims_valid = true;
+  }
+  return t->hdims.data();
+}
+
 void tensor_touch(sht_tensor* t, cudaStream_t s) {
   for (PoolBuf* b : {&t->d_bsizes, &t->d_bstart, &t->d_ids, &t->d_offsets, &t->d_dims, &t->d_data}) b->use_on(s);
 }
@@ -101,6 +114,7 @@ void tensor_touch(sht_tensor* t, cudaStream_t s) {
 // Pull the device index back to the host mirror when a device-side operation rebuilt it.
 void tensor_sync_host(sht_tensor* t, cudaStream_t s) {
   if (!t->host_stale) return;
+  t->hdims_valid = false;
   t->ids.resize(t->nblocks);
   t->offsets.resize(t->nblocks);
   if (t->nblocks) {
