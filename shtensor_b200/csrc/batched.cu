@@ -321,7 +321,19 @@ __global__ void k_emit_items(const int* __restrict__ idx, const long long* __res
   }
 }
 
-void device_work_list(sht_plan* p, int fixed_tm, int fixed_tn, bool per_class, cudaStream_t s) {
+// Up to eight device scalars gathered into one buffer for a single read-back.
+struct ScalarSrc {
+  const long long* p[8];
+  int n;
+};
+__global__ void k_collect(ScalarSrc src, long long* __restrict__ out) {
+  const int i = threadIdx.x;
+  if (i < src.n) out[i] = *src.p[i];
+}
+
+void device_work_list(sht_plan* p, int fixed_tm, int fixed_tn, bool per_class, cudaStream_t s,
+                      const long long* const* extra, long long* extra_out, int nextra) {
+  if (nextra > 4) fail(SHT_ERR_INVALID, "work list: at most four extra scalars");
   DevicePool* pool = p->ctx->pool.get();
   const long long nc = p->ncblk;
   p->bwork = p->bwork_touched = 0;
@@ -363,12 +375,25 @@ void device_work_list(sht_plan* p, int fixed_tm, int fixed_tn, bool per_class, c
   k_gather_tiles<<<grid_for(nc, 256), 256, 0, s>>>(idx2.as<int>(), tiles.as<long long>(), nc, tsorted.as<long long>());
   cub::DeviceScan::ExclusiveSum(tmp.ptr, tb2, tsorted.as<long long>(), off.as<long long>(), (int)nc, s);
   cub::DeviceReduce::Sum(tmp.ptr, tb3, ttiles.as<long long>(), sums.as<long long>(), (int)nc, s);
-  long long h[3];
-  SHT_CUDA(cudaMemcpyAsync(&h[0], off.as<long long>() + nc - 1, 8, cudaMemcpyDeviceToHost, s));
-  SHT_CUDA(cudaMemcpyAsync(&h[1], tsorted.as<long long>() + nc - 1, 8, cudaMemcpyDeviceToHost, s));
-  SHT_CUDA(cudaMemcpyAsync(&h[2], sums.ptr, 8, cudaMemcpyDeviceToHost, s));
-  SHT_CUDA(cudaStreamSynchronize(s));
-  plan_flops(p, s);  // the stream is idle after the reads above
+  // one read-back: the list's length and touched count, the plan's flop count (while it is
+  // still on the device) and the caller's extra scalars
+  ScalarSrc src{};
+  src.p[src.n++] = off.as<long long>() + nc - 1;
+  src.p[src.n++] = tsorted.as<long long>() + nc - 1;
+  src.p[src.n++] = sums.as<long long>();
+  const bool fl = p->flops_pending;
+  if (fl) src.p[src.n++] = p->d_flops.as<long long>();  // the double's bits
+  for (int i = 0; i < nextra; ++i) src.p[src.n++] = extra[i];
+  PoolBuf got(pool, 64, s);
+  k_collect<<<1, 32, 0, s>>>(src, got.as<long long>());
+  SHT_CUDA(cudaGetLastError());
+  long long h[8];
+  SHT_CUDA(cudaMemcpyAsync(h, got.ptr, src.n * 8, cudaMemcpyDeviceToHost, s));  // pageable: returns when done
+  if (fl) {
+    std::memcpy(&p->flops, &h[3], 8);
+    p->flops_pending = false;
+  }
+  for (int i = 0; i < nextra; ++i) extra_out[i] = h[src.n - nextra + i];
   const long long total = h[0] + h[1];
   if (total > (long long)INT32_MAX) fail(SHT_ERR_UNSUPPORTED, "work list above 2^31 tiles");
   p->bwork = total;

@@ -38,11 +38,11 @@ struct sht_plan {
   long long mf_elems = 0;
   // split path: INT8 slices (K-major rows), row / column exponents, error words
   sht::PoolBuf sp_a, sp_b, sp_ae, sp_be;
-  // one upload: per-block slice and exponent offsets of A and B, the slicer's int2 (block,
-  // first row) items of 32 rows, and the kernels' error words (zero)
+  // one upload: per block of A and of B its slice offset, exponent offset and first slicer
+  // item (items of 32 rows), and the kernels' error words (zero)
   sht::PoolBuf sp_meta;
-  long long *sp_aoff = nullptr, *sp_aeoff = nullptr, *sp_boff = nullptr, *sp_beoff = nullptr;
-  int2 *sp_aitems = nullptr, *sp_bitems = nullptr;
+  long long *sp_aoff = nullptr, *sp_aeoff = nullptr, *sp_aistart = nullptr;
+  long long *sp_boff = nullptr, *sp_beoff = nullptr, *sp_bistart = nullptr;
   int* sp_err = nullptr;
   long long sp_naitems = 0, sp_nbitems = 0;
   sht::PoolBuf sp_items, sp_pairs;    // per-tile and per-pair records of the split kernel
@@ -74,7 +74,9 @@ void cblock_stats(sht_plan* p, cudaStream_t s);
 double plan_flops(sht_plan* p, cudaStream_t s);
 // Cost-ordered work list (C block, tile, shape) on the device: fixed_shape >= 0 uses one
 // shape (tm x tn) for every block, otherwise per size class from class_shape (or the model).
-void device_work_list(sht_plan* p, int fixed_tm, int fixed_tn, bool per_class, cudaStream_t s);
+// extra (up to four device scalars) are read back with the list's own counts into extra_out.
+void device_work_list(sht_plan* p, int fixed_tm, int fixed_tn, bool per_class, cudaStream_t s,
+                      const long long* const* extra = nullptr, long long* extra_out = nullptr, int nextra = 0);
 void plan_execute(sht_plan* p, double alpha, double beta, cudaStream_t s);
 void batched_prepare(sht_plan* p, cudaStream_t s);
 void batched_execute(sht_plan* p, const SparseArgs& g, long long nwork_plain, cudaStream_t s);

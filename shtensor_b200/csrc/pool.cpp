@@ -64,8 +64,8 @@ DevicePool::EventRef DevicePool::record_event(cudaStream_t stream) {
     spare_events_.push_back(e);
     fail(SHT_ERR_CUDA, std::string("cudaEventRecord in pool free: ") + cudaGetErrorString(rc));
   }
-  return EventRef(new cudaEvent_t(e), [this](cudaEvent_t* p) {
-    spare_events_.push_back(*p);
+  return EventRef(new PoolEvent{e, stream}, [this](PoolEvent* p) {
+    spare_events_.push_back(p->event);
     delete p;
   });
 }
@@ -75,12 +75,13 @@ DevicePool::EventRef DevicePool::record_event(cudaStream_t stream) {
 void DevicePool::prune(std::vector<EventRef>& v) {
   std::sort(v.begin(), v.end());
   v.erase(std::unique(v.begin(), v.end()), v.end());
-  v.erase(std::remove_if(v.begin(), v.end(), [](const EventRef& e) { return cudaEventQuery(*e) == cudaSuccess; }),
+  v.erase(std::remove_if(v.begin(), v.end(), [](const EventRef& e) { return cudaEventQuery(e->event) == cudaSuccess; }),
           v.end());
 }
 
 void DevicePool::wait_pending(const Chunk& c, cudaStream_t stream) {
-  for (const EventRef& ev : c.pending) SHT_CUDA(cudaStreamWaitEvent(stream, *ev, 0));
+  for (const EventRef& ev : c.pending)
+    if (ev->stream != stream) SHT_CUDA(cudaStreamWaitEvent(stream, ev->event, 0));
 }
 
 bool DevicePool::owns(const void* p) const {

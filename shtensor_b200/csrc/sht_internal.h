@@ -86,7 +86,13 @@ class DevicePool {
   bool owns(const void* p) const;
 
  private:
-  using EventRef = std::shared_ptr<cudaEvent_t>;
+  // an event recorded at a free, with the stream it was recorded on (an allocation on that
+  // same stream is ordered after the free already and needs no wait)
+  struct PoolEvent {
+    cudaEvent_t event;
+    cudaStream_t stream;
+  };
+  using EventRef = std::shared_ptr<PoolEvent>;
   struct Chunk {
     size_t size = 0;  // data bytes (header excluded)
     bool free = true;

@@ -65,7 +65,8 @@ __host__ __device__ __forceinline__ int slab_offset(int r, int k) {
   return (r >> 3) * 256 + (k >> 4) * 128 + (r & 7) * 16 + (k & 15);
 }
 
-// One warp per item of 32 rows of one block (lane = row): the row maximum gives the row's
+// One warp per item of 32 rows of one block (lane = row; items are numbered block after block,
+// istart[b] the first item of block b): the row maximum gives the row's
 // exponent (rows padded up to the tile height R get 0), then the S int8 slices of the row
 // go out in tile order: out[((tile * ksteps + ks) * S + t) * R * 32 + slab_offset(row % R, k)].
 // Rows past the block and k past K are zero.
@@ -74,14 +75,19 @@ __global__ void __launch_bounds__(256) k_slice(const double* __restrict__ src, c
                                                const long long* __restrict__ out_off,
                                                const long long* __restrict__ exp_off, signed char* __restrict__ out,
                                                short* __restrict__ expo, double scale, int S, int R,
-                                               const int2* __restrict__ items, long long nitems,
-                                               int* __restrict__ bad) {
+                                               const long long* __restrict__ istart, long long nblocks,
+                                               long long nitems, int* __restrict__ bad) {
   const int lane = threadIdx.x & 31;
   const long long nwarps = (long long)gridDim.x * (blockDim.x >> 5);
   for (long long it = blockIdx.x * (long long)(blockDim.x >> 5) + (threadIdx.x >> 5); it < nitems; it += nwarps) {
-    const int2 item = items[it];
-    const long long b = item.x;
-    const int r = item.y + lane;
+    // the block holding item it: the last block whose first item is <= it
+    long long lo = 0, hi = nblocks;
+    while (hi - lo > 1) {
+      const long long mid = (lo + hi) >> 1;
+      if (istart[mid] <= it) lo = mid; else hi = mid;
+    }
+    const long long b = lo;
+    const int r = (int)(it - istart[b]) * 32 + lane;
     const int* d = dims + b * order;
     int st[kMaxOrder];
     block_strides(d, order, st);
@@ -656,12 +662,13 @@ static ModeMap modes_of(const std::vector<int>& v) {
 // Per block: byte offset of its slices (tiles of R rows) and offset of its exponents (rows
 // padded to a multiple of R), plus the slicer's items of 32 rows.  Groups hold exact INT32
 // sums of up to S products of |s| <= 127 per k, so K is limited to keep them below 2^31.
-static void slice_layout(sht_tensor* T, const std::vector<int>& free_modes, const std::vector<int>& k_modes,
-                         int S, int R, long long* off, long long* eoff, long long& total, long long& etotal,
-                         std::vector<int2>& items) {
+template <int R>
+static void slice_layout(sht_tensor* T, const std::vector<int>& free_modes, const std::vector<int>& k_modes, int S,
+                         long long* off, long long* eoff, long long* istart, long long& total, long long& etotal,
+                         long long& nitems) {
   const long long n = T->nblocks;
   const int* dims = tensor_host_dims(T);
-  total = etotal = 0;
+  total = etotal = nitems = 0;
   for (long long b = 0; b < n; ++b) {
     const int* d = dims + b * T->order;
     long long m = 1, K = 1;
@@ -673,9 +680,10 @@ static void slice_layout(sht_tensor* T, const std::vector<int>& free_modes, cons
     if ((long long)S * mp * Kp >= (1LL << 31)) fail(SHT_ERR_UNSUPPORTED, "block slices above 2^31 bytes");
     off[b] = total;
     eoff[b] = etotal;
+    istart[b] = nitems;
     total += (long long)S * mp * Kp;  // a multiple of 1 KB: every block stays aligned for bulk copies
     etotal += mp;
-    for (long long r0 = 0; r0 < mp; r0 += 32) items.push_back(make_int2((int)b, (int)r0));
+    nitems += mp / 32;  // the slicer's items: 32 rows each
   }
 }
 
@@ -691,18 +699,15 @@ void split_layout(sht_plan* p, int S, cudaStream_t s) {
   DevicePool* pool = p->ctx->pool.get();
   p->split_slices = S;
   const long long nA = p->A->nblocks, nB = p->B->nblocks;
-  // host image of sp_meta: [A offsets | A exponent offsets | B offsets | B exponent offsets |
-  // error words (32 x 8 bytes) | A items | B items], 8-byte words
-  std::vector<long long> meta((size_t)(2 * nA + 2 * nB + 32));
-  std::vector<int2> ia, ib;
-  long long at, aet, bt, bet;
-  slice_layout(p->A, p->maps.rowA, p->maps.colA, S, kSplitM, meta.data(), meta.data() + nA, at, aet, ia);
-  slice_layout(p->B, p->maps.colB, p->maps.rowB, S, kSplitN, meta.data() + 2 * nA, meta.data() + 2 * nA + nB, bt,
-               bet, ib);
-  const size_t head = meta.size();
-  meta.resize(head + ia.size() + ib.size());
-  std::memcpy(meta.data() + head, ia.data(), ia.size() * sizeof(int2));
-  std::memcpy(meta.data() + head + ia.size(), ib.data(), ib.size() * sizeof(int2));
+  // host image of sp_meta, 8-byte words: per A block its slice offset, exponent offset and
+  // first slicer item, the same per B block, then the error words (32 x 8 bytes, zero)
+  std::vector<long long> meta((size_t)(3 * nA + 3 * nB + 32));
+  long long at, aet, bt, bet, nia, nib;
+  slice_layout<kSplitM>(p->A, p->maps.rowA, p->maps.colA, S, meta.data(), meta.data() + nA, meta.data() + 2 * nA, at,
+                        aet, nia);
+  long long* mb = meta.data() + 3 * nA;
+  slice_layout<kSplitN>(p->B, p->maps.colB, p->maps.rowB, S, mb, mb + nB, mb + 2 * nB, bt, bet, nib);
+  trace("split: slice layout (host)", s);
   p->sp_a = PoolBuf(pool, std::max(at, 16LL), s);
   p->sp_b = PoolBuf(pool, std::max(bt, 16LL), s);
   p->sp_ae = PoolBuf(pool, std::max(aet, 1LL) * 2, s);
@@ -711,13 +716,14 @@ void split_layout(sht_plan* p, int S, cudaStream_t s) {
   long long* dm = p->sp_meta.as<long long>();
   p->sp_aoff = dm;
   p->sp_aeoff = dm + nA;
-  p->sp_boff = dm + 2 * nA;
-  p->sp_beoff = dm + 2 * nA + nB;
-  p->sp_err = reinterpret_cast<int*>(dm + 2 * nA + 2 * nB);
-  p->sp_aitems = reinterpret_cast<int2*>(dm + head);
-  p->sp_bitems = reinterpret_cast<int2*>(dm + head + ia.size());
-  p->sp_naitems = (long long)ia.size();
-  p->sp_nbitems = (long long)ib.size();
+  p->sp_aistart = dm + 2 * nA;
+  p->sp_boff = dm + 3 * nA;
+  p->sp_beoff = dm + 3 * nA + nB;
+  p->sp_bistart = dm + 3 * nA + 2 * nB;
+  p->sp_err = reinterpret_cast<int*>(dm + 3 * nA + 3 * nB);
+  p->sp_naitems = nia;
+  p->sp_nbitems = nib;
+  trace("split: slice buffers", s);
   // one copy (from pageable memory it has consumed its source when it returns)
   SHT_CUDA(cudaMemcpyAsync(dm, meta.data(), meta.size() * 8, cudaMemcpyHostToDevice, s));
   trace("split: slice layout", s);
@@ -725,36 +731,32 @@ void split_layout(sht_plan* p, int S, cudaStream_t s) {
 
 void split_records(sht_plan* p, cudaStream_t s) {
   DevicePool* pool = p->ctx->pool.get();
-  // work list: 128 x 32 tiles of every C block, heaviest blocks first, with per-tile and
-  // per-pair records so that the kernel reads each with one load
-  device_work_list(p, kSplitM, kSplitN, false, s);
-  trace("split: work list", s);
   // row / column offset tables of the C blocks: starts from a scan of the blocks' row and
-  // column counts (rounded up to 4 so that every tile's slice of a table is 16-byte aligned)
+  // column counts (rounded up to 4 so that every tile's slice of a table is 16-byte aligned);
+  // the totals come back with the work list's counts
   const sht_tensor* C = p->C;
   const long long nc = C->nblocks;
   PoolBuf drb(pool, std::max(nc, 1LL) * 8, s), dcb(pool, std::max(nc, 1LL) * 8, s);
+  PoolBuf rm(pool, std::max(nc, 1LL) * 8, s), rn(pool, std::max(nc, 1LL) * 8, s);
   long long rtot = 0, ctot = 0;
   if (nc > 0) {
-    PoolBuf rm(pool, nc * 8, s), rn(pool, nc * 8, s);
     k_round4<<<grid_for(nc, 256), 256, 0, s>>>(p->d_cm.as<int>(), p->d_cn.as<int>(), nc, rm.as<long long>(),
                                                rn.as<long long>());
     size_t tb = 0;
     cub::DeviceScan::ExclusiveSum(nullptr, tb, rm.as<long long>(), drb.as<long long>(), (int)nc, s);
-    {
-      PoolBuf tmp(pool, tb, s);
-      cub::DeviceScan::ExclusiveSum(tmp.ptr, tb, rm.as<long long>(), drb.as<long long>(), (int)nc, s);
-      cub::DeviceScan::ExclusiveSum(tmp.ptr, tb, rn.as<long long>(), dcb.as<long long>(), (int)nc, s);
-    }
-    long long h[4];
-    SHT_CUDA(cudaMemcpyAsync(&h[0], drb.as<long long>() + nc - 1, 8, cudaMemcpyDeviceToHost, s));
-    SHT_CUDA(cudaMemcpyAsync(&h[1], rm.as<long long>() + nc - 1, 8, cudaMemcpyDeviceToHost, s));
-    SHT_CUDA(cudaMemcpyAsync(&h[2], dcb.as<long long>() + nc - 1, 8, cudaMemcpyDeviceToHost, s));
-    SHT_CUDA(cudaMemcpyAsync(&h[3], rn.as<long long>() + nc - 1, 8, cudaMemcpyDeviceToHost, s));
-    SHT_CUDA(cudaStreamSynchronize(s));
-    rtot = h[0] + h[1];
-    ctot = h[2] + h[3];
+    PoolBuf tmp(pool, tb, s);
+    cub::DeviceScan::ExclusiveSum(tmp.ptr, tb, rm.as<long long>(), drb.as<long long>(), (int)nc, s);
+    cub::DeviceScan::ExclusiveSum(tmp.ptr, tb, rn.as<long long>(), dcb.as<long long>(), (int)nc, s);
   }
+  // work list: 128 x 32 tiles of every C block, heaviest blocks first, with per-tile and
+  // per-pair records so that the kernel reads each with one load
+  const long long* extra[4] = {drb.as<long long>() + nc - 1, rm.as<long long>() + nc - 1,
+                               dcb.as<long long>() + nc - 1, rn.as<long long>() + nc - 1};
+  long long h[4] = {0, 0, 0, 0};
+  device_work_list(p, kSplitM, kSplitN, false, s, extra, h, nc > 0 ? 4 : 0);
+  rtot = h[0] + h[1];
+  ctot = h[2] + h[3];
+  trace("split: work list", s);
   if (rtot >= (1LL << 31) || ctot >= (1LL << 31)) fail(SHT_ERR_UNSUPPORTED, "split mode: C row / column tables above 2^31");
   // a tile reads a full 128 rows / 32 columns: slack past the last block
   p->sp_rowtab = PoolBuf(pool, (rtot + kSplitM) * 4, s);
@@ -818,14 +820,14 @@ void split_slice(sht_plan* p, double alpha, cudaStream_t s) {
       k_slice<<<(int)std::min((p->sp_naitems + 7) / 8, cap), 256, 0, s>>>(
           p->A->d_data.as<double>(), p->A->d_offsets.as<long long>(), p->A->d_dims.as<int>(), p->A->order,
           modes_of(p->maps.rowA), modes_of(p->maps.colA), p->sp_aoff, p->sp_aeoff,
-          p->sp_a.as<signed char>(), p->sp_ae.as<short>(), alpha, S, kSplitM, p->sp_aitems,
-          p->sp_naitems, p->sp_err + 1);
+          p->sp_a.as<signed char>(), p->sp_ae.as<short>(), alpha, S, kSplitM, p->sp_aistart,
+          p->A->nblocks, p->sp_naitems, p->sp_err + 1);
     if (p->sp_nbitems)
       k_slice<<<(int)std::min((p->sp_nbitems + 7) / 8, cap), 256, 0, s>>>(
           p->B->d_data.as<double>(), p->B->d_offsets.as<long long>(), p->B->d_dims.as<int>(), p->B->order,
           modes_of(p->maps.colB), modes_of(p->maps.rowB), p->sp_boff, p->sp_beoff,
-          p->sp_b.as<signed char>(), p->sp_be.as<short>(), 1.0, S, kSplitN, p->sp_bitems, p->sp_nbitems,
-          p->sp_err + 1);
+          p->sp_b.as<signed char>(), p->sp_be.as<short>(), 1.0, S, kSplitN, p->sp_bistart, p->B->nblocks,
+          p->sp_nbitems, p->sp_err + 1);
     SHT_CUDA(cudaGetLastError());
   }
 }
