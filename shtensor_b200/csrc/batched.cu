@@ -321,19 +321,20 @@ __global__ void k_emit_items(const int* __restrict__ idx, const long long* __res
   }
 }
 
-// Up to eight device scalars gathered into one buffer for a single read-back.
+// Up to eight device scalars (each a value or the sum of two) gathered into one buffer for a
+// single read-back.
 struct ScalarSrc {
-  const long long* p[8];
+  DevSum v[8];
   int n;
 };
 __global__ void k_collect(ScalarSrc src, long long* __restrict__ out) {
   const int i = threadIdx.x;
-  if (i < src.n) out[i] = *src.p[i];
+  if (i < src.n) out[i] = *src.v[i].a + (src.v[i].b ? *src.v[i].b : 0);
 }
 
-void device_work_list(sht_plan* p, int fixed_tm, int fixed_tn, bool per_class, cudaStream_t s,
-                      const long long* const* extra, long long* extra_out, int nextra) {
-  if (nextra > 4) fail(SHT_ERR_INVALID, "work list: at most four extra scalars");
+void device_work_list(sht_plan* p, int fixed_tm, int fixed_tn, bool per_class, cudaStream_t s, const DevSum* extra,
+                      long long* extra_out, int nextra) {
+  if (nextra > 3) fail(SHT_ERR_INVALID, "work list: at most three extra scalars");
   DevicePool* pool = p->ctx->pool.get();
   const long long nc = p->ncblk;
   p->bwork = p->bwork_touched = 0;
@@ -378,26 +379,40 @@ void device_work_list(sht_plan* p, int fixed_tm, int fixed_tn, bool per_class, c
   // one read-back: the list's length and touched count, the plan's flop count (while it is
   // still on the device) and the caller's extra scalars
   ScalarSrc src{};
-  src.p[src.n++] = off.as<long long>() + nc - 1;
-  src.p[src.n++] = tsorted.as<long long>() + nc - 1;
-  src.p[src.n++] = sums.as<long long>();
+  src.v[src.n++] = {off.as<long long>() + nc - 1, tsorted.as<long long>() + nc - 1};
+  src.v[src.n++] = {sums.as<long long>(), nullptr};
   const bool fl = p->flops_pending;
-  if (fl) src.p[src.n++] = p->d_flops.as<long long>();  // the double's bits
-  for (int i = 0; i < nextra; ++i) src.p[src.n++] = extra[i];
+  if (fl) src.v[src.n++] = {p->d_flops.as<long long>(), nullptr};  // the double's bits
+  const bool npc = p->d_npairs.ptr != nullptr;
+  const int inp = src.n;
+  if (npc) src.v[src.n++] = {p->d_npairs.as<long long>(), nullptr};  // the device's pair count
+  const bool msc = p->d_missing.ptr != nullptr;
+  const int ims = src.n;
+  if (msc) src.v[src.n++] = {p->d_missing.as<long long>(), nullptr};  // product blocks not in C
+  for (int i = 0; i < nextra; ++i) src.v[src.n++] = extra[i];
   PoolBuf got(pool, 64, s);
   k_collect<<<1, 32, 0, s>>>(src, got.as<long long>());
   SHT_CUDA(cudaGetLastError());
   long long h[8];
   SHT_CUDA(cudaMemcpyAsync(h, got.ptr, src.n * 8, cudaMemcpyDeviceToHost, s));  // pageable: returns when done
   if (fl) {
-    std::memcpy(&p->flops, &h[3], 8);
+    std::memcpy(&p->flops, &h[2], 8);
     p->flops_pending = false;
   }
   for (int i = 0; i < nextra; ++i) extra_out[i] = h[src.n - nextra + i];
-  const long long total = h[0] + h[1];
+  if (msc) {
+    p->d_missing = PoolBuf();
+    if (h[ims] != 0) throw PatternGrew{};  // the build assumed C's pattern: redo it
+  }
+  if (npc) {
+    // the pair list was sized from the host patterns: the device must have found as many
+    if (h[inp] != p->npairs) fail(SHT_ERR_STATE, "pair count of the host patterns differs from the device's");
+    p->d_npairs = PoolBuf();
+  }
+  const long long total = h[0];
   if (total > (long long)INT32_MAX) fail(SHT_ERR_UNSUPPORTED, "work list above 2^31 tiles");
   p->bwork = total;
-  p->bwork_touched = h[2];
+  p->bwork_touched = h[1];
   p->d_bwork = PoolBuf(pool, std::max(total, 1LL) * sizeof(int4), s);
   k_emit_items<<<grid_for(nc, 128), 128, 0, s>>>(idx2.as<int>(), tsorted.as<long long>(), off.as<long long>(),
                                                   shape.as<int>(), nc, p->d_bwork.as<int4>());

@@ -55,8 +55,14 @@ static void contract_split(sht_plan* p, double alpha, double beta, cudaStream_t 
   split_slice(p, alpha, s);
   trace("contract: slicer launched", s);
   SHT_CUDA(cudaStreamWaitEvent(ps, lane.lane.start, 0));
-  plan_build(p, ps);
-  split_records(p, ps);
+  try {
+    plan_build(p, ps, true);
+    split_records(p, ps);
+  } catch (const PatternGrew&) {
+    // the product adds blocks to C: build again, growing C's pattern
+    plan_build(p, ps, false);
+    split_records(p, ps);
+  }
   SHT_CUDA(cudaEventRecord(lane.lane.done, ps));
   SHT_CUDA(cudaStreamWaitEvent(s, lane.lane.done, 0));
   plan_touch(p, s);

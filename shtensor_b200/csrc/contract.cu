@@ -393,8 +393,7 @@ sht_plan* plan_init(sht_ctx* ctx, const std::string& expr, sht_tensor* A, sht_te
   for (sht_tensor* t : {A, B, C}) {
     tensor_touch(t, s);
     tensor_sync_host(t, s);
-    for (int64_t id : t->ids)
-      if (id < 0) fail(SHT_ERR_STATE, "tensor has filtered blocks that were not compressed");
+    if (t->has_marked) fail(SHT_ERR_STATE, "tensor has filtered blocks that were not compressed");
   }
   auto p = std::make_unique<sht_plan>();
   p->keep = ctx->pool;
@@ -412,7 +411,7 @@ sht_plan* plan_init(sht_ctx* ctx, const std::string& expr, sht_tensor* A, sht_te
   return p.release();
 }
 
-void plan_build(sht_plan* p, cudaStream_t s) {
+void plan_build(sht_plan* p, cudaStream_t s, bool speculate) {
   const double t0 = now_ms();
   sht_ctx* ctx = p->ctx;
   sht_tensor *A = p->A, *B = p->B, *C = p->C;
@@ -445,6 +444,25 @@ void plan_build(sht_plan* p, cudaStream_t s) {
   for (int d = 0; d < C->order; ++d) cgrid *= C->nblk[d];
   if (cgrid > 9.0e18L) fail(SHT_ERR_UNSUPPORTED, "C block grid too large");
 
+  // Without screening the pair count follows from the host patterns (per contracted key the
+  // number of B blocks, summed over A's blocks), so the device count need not be read back.
+  long long np_host = -1;
+  if (!(eps > 0.0) && kspan <= (1ULL << 16) && nA > 0 && nB > 0) {
+    const int* xa = tensor_host_coords(A);
+    const int* xb = tensor_host_coords(B);
+    std::vector<long long> nbk(kspan, 0);
+    for (long long b = 0; b < nB; ++b) {
+      long long k = 0;
+      for (int t = 0; t < kb.nk; ++t) k += xb[b * B->order + kb.kmode[t]] * kb.kstride[t];
+      nbk[k]++;
+    }
+    np_host = 0;
+    for (long long a = 0; a < nA; ++a) {
+      long long k = 0;
+      for (int t = 0; t < ka.nk; ++t) k += xa[a * A->order + ka.kmode[t]] * ka.kstride[t];
+      np_host += nbk[k];
+    }
+  }
   long long np = 0;
   PoolBuf pc_sorted;
   if (nA > 0 && nB > 0) {
@@ -492,7 +510,14 @@ void plan_build(sht_plan* p, cudaStream_t s) {
       PoolBuf tmp(pool, tb, s);
       cub::DeviceScan::InclusiveSum(tmp.ptr, tb, cnt.as<long long>(), off.as<long long>(), (int)nA, s);
     }
-    np = d2h_scalar<long long>(off.as<long long>() + nA - 1, s);
+    if (np_host >= 0) {
+      // checked against the device's count at the next read-back (work list)
+      np = np_host;
+      p->d_npairs = PoolBuf(pool, 8, s);
+      SHT_CUDA(cudaMemcpyAsync(p->d_npairs.ptr, off.as<long long>() + nA - 1, 8, cudaMemcpyDeviceToDevice, s));
+    } else {
+      np = d2h_scalar<long long>(off.as<long long>() + nA - 1, s);
+    }
     if (np > (long long)INT32_MAX) fail(SHT_ERR_UNSUPPORTED, "more than 2^31 block pairs");
     if (np > 0) {
       PoolBuf pc(pool, np * 8, s), pa(pool, np * 4, s), pb(pool, np * 4, s);
@@ -534,7 +559,12 @@ void plan_build(sht_plan* p, cudaStream_t s) {
     k_count_missing<<<grid_for(np, 256), 256, 0, s>>>(pc_sorted.as<long long>(), np, C->d_ids.as<long long>(),
                                                        C->nblocks, miss.as<unsigned long long>());
     SHT_CUDA(cudaGetLastError());
-    grow = d2h_scalar<unsigned long long>(miss.ptr, s) > 0;
+    if (speculate) {
+      p->d_missing = std::move(miss);
+      grow = false;
+    } else {
+      grow = d2h_scalar<unsigned long long>(miss.ptr, s) > 0;
+    }
   }
   if (grow) {
     uids = PoolBuf(pool, np * 8, s);
@@ -658,6 +688,12 @@ void build_work(sht_plan* p, int TM, int TN, cudaStream_t s) {
                                                  ou.as<long long>(), nt, p->d_work.as<int2>());
   SHT_CUDA(cudaGetLastError());
   plan_flops(p, s);  // the stream is idle after the reads above
+  if (p->d_npairs.ptr) {
+    // the pair list was sized from the host patterns: the device must have found as many
+    if (d2h_scalar<long long>(p->d_npairs.ptr, s) != p->npairs)
+      fail(SHT_ERR_STATE, "pair count of the host patterns differs from the device's");
+    p->d_npairs = PoolBuf();
+  }
   p->nwork_touched = nt;
   p->nwork = nt + nu;
   p->work_tm = TM;

@@ -16,6 +16,8 @@ struct sht_plan {
   double eps = 0.0;                 // screening threshold and norm of the pair list
   sht_norm norm = SHT_NORM_FROBENIUS;
   sht::PoolBuf d_flops;             // device total of the flop count until it is read
+  sht::PoolBuf d_npairs;            // device pair count, when the host's sized the pair list
+  sht::PoolBuf d_missing;           // product blocks absent from C, when the build assumed none
   bool flops_pending = false;       // d_flops not yet copied into flops
   int shape = 0, work_tm = 64, work_tn = 64;
   sht::PoolBuf d_pair_a, d_pair_b;  // int32 storage indices into A / B, canonical order
@@ -66,7 +68,11 @@ sht_plan* plan_create(sht_ctx* ctx, const std::string& expr, sht_tensor* A, sht_
 // host patterns back on s), then the pair list, result pattern and per-block statistics on s
 sht_plan* plan_init(sht_ctx* ctx, const std::string& expr, sht_tensor* A, sht_tensor* B, sht_tensor* C,
                     double eps, sht_norm norm, sht_mode mode, cudaStream_t s);
-void plan_build(sht_plan* p, cudaStream_t s);
+// speculate: when C already has a pattern, assume the product adds no block to it and check
+// that at the work list's read-back (device_work_list throws PatternGrew if it did), which
+// saves a synchronization when C is contracted into repeatedly.
+void plan_build(sht_plan* p, cudaStream_t s, bool speculate = false);
+struct PatternGrew {};
 void build_work(sht_plan* p, int TM, int TN, cudaStream_t s);
 void cblock_stats(sht_plan* p, cudaStream_t s);
 // The plan's flop count; the first call after planning copies it from the device (a sync),
@@ -74,9 +80,14 @@ void cblock_stats(sht_plan* p, cudaStream_t s);
 double plan_flops(sht_plan* p, cudaStream_t s);
 // Cost-ordered work list (C block, tile, shape) on the device: fixed_shape >= 0 uses one
 // shape (tm x tn) for every block, otherwise per size class from class_shape (or the model).
-// extra (up to four device scalars) are read back with the list's own counts into extra_out.
+// A device scalar, or the sum of two (b may be null), for a read-back.
+struct DevSum {
+  const long long* a;
+  const long long* b;
+};
+// extra (up to three device scalars) are read back with the list's own counts into extra_out.
 void device_work_list(sht_plan* p, int fixed_tm, int fixed_tn, bool per_class, cudaStream_t s,
-                      const long long* const* extra = nullptr, long long* extra_out = nullptr, int nextra = 0);
+                      const DevSum* extra = nullptr, long long* extra_out = nullptr, int nextra = 0);
 void plan_execute(sht_plan* p, double alpha, double beta, cudaStream_t s);
 void batched_prepare(sht_plan* p, cudaStream_t s);
 void batched_execute(sht_plan* p, const SparseArgs& g, long long nwork_plain, cudaStream_t s);

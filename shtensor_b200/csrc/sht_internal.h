@@ -202,10 +202,12 @@ struct sht_tensor {
   // host index (authoritative unless host_stale)
   std::vector<int64_t> ids, offsets, rows;
   bool host_stale = false;
-  // per-block extents (nblocks x order) of the host index, computed on first use after the
-  // host index changes (tensor_host_dims)
-  std::vector<int> hdims;
+  bool has_marked = false;  // the host index holds filtered (negative) ids
+  // per-block extents and block-grid coordinates (nblocks x order each) of the host index,
+  // computed on first use after the host index changes (tensor_host_dims, tensor_host_coords)
+  std::vector<int> hdims, hcoords;
   bool hdims_valid = false;
+  std::mutex hmu;  // the serving loop's planner threads share input tensors
   int64_t nblocks = 0, nnz = 0;
   // device arrays
   sht::PoolBuf d_bsizes;   // int32, concatenated per mode
@@ -228,6 +230,7 @@ void tensor_set_index(sht_tensor* t, std::vector<int64_t>&& ids, cudaStream_t s)
 void tensor_sync_host(sht_tensor* t, cudaStream_t s);
 // per-block extents of the host index, nblocks x order (the host index must be current)
 const int* tensor_host_dims(sht_tensor* t);
+const int* tensor_host_coords(sht_tensor* t);
 void tensor_upload_index(sht_tensor* t, cudaStream_t s);
 void tensor_norms_device(sht_tensor* t, sht_norm norm, double* d_out, cudaStream_t s);
 // Record that `s` uses the tensor's device buffers: when they are freed, reuse of the memory

@@ -750,12 +750,12 @@ void split_records(sht_plan* p, cudaStream_t s) {
   }
   // work list: 128 x 32 tiles of every C block, heaviest blocks first, with per-tile and
   // per-pair records so that the kernel reads each with one load
-  const long long* extra[4] = {drb.as<long long>() + nc - 1, rm.as<long long>() + nc - 1,
-                               dcb.as<long long>() + nc - 1, rn.as<long long>() + nc - 1};
-  long long h[4] = {0, 0, 0, 0};
-  device_work_list(p, kSplitM, kSplitN, false, s, extra, h, nc > 0 ? 4 : 0);
-  rtot = h[0] + h[1];
-  ctot = h[2] + h[3];
+  const DevSum extra[2] = {{drb.as<long long>() + nc - 1, rm.as<long long>() + nc - 1},
+                           {dcb.as<long long>() + nc - 1, rn.as<long long>() + nc - 1}};
+  long long h[2] = {0, 0};
+  device_work_list(p, kSplitM, kSplitN, false, s, extra, h, nc > 0 ? 2 : 0);
+  rtot = h[0];
+  ctot = h[1];
   trace("split: work list", s);
   if (rtot >= (1LL << 31) || ctot >= (1LL << 31)) fail(SHT_ERR_UNSUPPORTED, "split mode: C row / column tables above 2^31");
   // a tile reads a full 128 rows / 32 columns: slack past the last block

@@ -65,7 +65,11 @@ void block_dims_sizes(const sht_tensor* t, const long long* ids, long long n, in
 void tensor_set_index(sht_tensor* t, std::vector<int64_t>&& ids, cudaStream_t s) {
   DevicePool* pool = t->ctx->pool.get();
   t->ids = std::move(ids);
-  t->hdims_valid = false;
+  t->has_marked = false;
+  {
+    std::lock_guard<std::mutex> lk(t->hmu);
+    t->hdims_valid = false;
+  }
   t->nblocks = static_cast<int64_t>(t->ids.size());
   t->offsets.resize(t->ids.size());
   int64_t off = 0;
@@ -95,16 +99,31 @@ void tensor_set_index(sht_tensor* t, std::vector<int64_t>&& ids, cudaStream_t s)
   SHT_CUDA(cudaStreamSynchronize(s));
 }
 
-const int* tensor_host_dims(sht_tensor* t) {
-  if (!t->hdims_valid) {
-    t->hdims.resize(std::max<size_t>(t->ids.size() * t->order, 1));
-    for (size_t b = 0; b < t->ids.size(); ++b) {
-      const int64_t id = t->ids[b] >= 0 ? t->ids[b] : -(t->ids[b] + 1);  // marked ids are -(id)-1
-      for (int d = 0; d < t->order; ++d) t->hdims[b * t->order + d] = t->bs[d][(id / t->gstride[d]) % t->nblk[d]];
+static void host_index_arrays(sht_tensor* t) {
+  std::lock_guard<std::mutex> lk(t->hmu);
+  if (t->hdims_valid) return;
+  const size_t n = std::max<size_t>(t->ids.size() * t->order, 1);
+  t->hdims.resize(n);
+  t->hcoords.resize(n);
+  for (size_t b = 0; b < t->ids.size(); ++b) {
+    const int64_t id = t->ids[b] >= 0 ? t->ids[b] : -(t->ids[b] + 1);  // marked ids are -(id)-1
+    for (int d = 0; d < t->order; ++d) {
+      const int x = (int)((id / t->gstride[d]) % t->nblk[d]);
+      t->hcoords[b * t->order + d] = x;
+      t->hdims[b * t->order + d] = t->bs[d][x];
     }
-    t->hdims_valid = true;
   }
+  t->hdims_valid = true;
+}
+
+const int* tensor_host_dims(sht_tensor* t) {
+  host_index_arrays(t);
   return t->hdims.data();
+}
+
+const int* tensor_host_coords(sht_tensor* t) {
+  host_index_arrays(t);
+  return t->hcoords.data();
 }
 
 void tensor_touch(sht_tensor* t, cudaStream_t s) {
@@ -114,7 +133,10 @@ void tensor_touch(sht_tensor* t, cudaStream_t s) {
 // Pull the device index back to the host mirror when a device-side operation rebuilt it.
 void tensor_sync_host(sht_tensor* t, cudaStream_t s) {
   if (!t->host_stale) return;
-  t->hdims_valid = false;
+  {
+    std::lock_guard<std::mutex> lk(t->hmu);
+    t->hdims_valid = false;
+  }
   t->ids.resize(t->nblocks);
   t->offsets.resize(t->nblocks);
   if (t->nblocks) {
@@ -124,7 +146,12 @@ void tensor_sync_host(sht_tensor* t, cudaStream_t s) {
   SHT_CUDA(cudaStreamSynchronize(s));
   t->rows.assign(t->nblk[0], 0);
   std::vector<int64_t> cnt(t->nblk[0], 0);
-  for (int64_t id : t->ids) cnt[(id >= 0 ? id : -(id + 1)) % t->nblk[0]]++;  // marked ids are -(id)-1
+  bool marked = false;
+  for (int64_t id : t->ids) {
+    marked = marked || id < 0;
+    cnt[(id >= 0 ? id : -(id + 1)) % t->nblk[0]]++;  // marked ids are -(id)-1
+  }
+  t->has_marked = marked;
   int64_t acc = 0;
   for (int r = 0; r < t->nblk[0]; ++r) { t->rows[r] = acc; acc += cnt[r]; }
   t->host_stale = false;

@@ -144,3 +144,27 @@ def test_split_long_contracted_extent(ctx):
     w = W.Workload("long_k", "ik, kj -> ij", A, B, W.empty_tensor([bi, bj]))
     errs = per_block_errors(ctx, w)
     assert max(e[0] for e in errs) <= REL_TOL, errs
+
+
+def test_split_contract_grows_then_reuses_pattern(ctx):
+    # sht_contract plans assuming C's stored pattern covers the product and checks that at the
+    # work list; a C holding only part of the product takes the second build, which grows it;
+    # the next contraction into the grown C keeps the assumption
+    w = W.c1(seed=7, scale=0.2, occupancy=0.3)
+    rng = np.random.default_rng(8)
+    Ch = W.build_tensor(rng, w.C.block_sizes, lambda c: rng.random(len(c[0])) < 0.2, None, "normal")
+    A, B, C = dev(ctx, w.A), dev(ctx, w.B), dev(ctx, Ch)
+    sht.contract(ctx, w.expr, 0.5, A, B, 1.5, C, mode=sht.Mode.SPLIT)
+    want = oracle.contract(w.expr, 0.5, host(w.A), host(w.B), 1.5, host(Ch))
+    ids, offs, _ = C.get_sparse_info()
+    assert np.array_equal(ids, want.C.ids) and np.array_equal(offs, want.C.offsets)
+    got = C.download()
+    assert np.linalg.norm(got - want.C.data) <= REL_TOL * np.linalg.norm(want.C.data)
+    # again into the grown C: the pattern holds every product block now
+    Cg = oracle.HostTensor(w.C.block_sizes, ids, offs, got)
+    sht.contract(ctx, w.expr, 1.0, A, B, -1.0, C, mode=sht.Mode.SPLIT)
+    want2 = oracle.contract(w.expr, 1.0, host(w.A), host(w.B), -1.0, Cg)
+    ids2, _, _ = C.get_sparse_info()
+    assert np.array_equal(ids2, ids)
+    got2 = C.download()
+    assert np.linalg.norm(got2 - want2.C.data) <= REL_TOL * max(np.linalg.norm(want2.C.data), 1e-300)
