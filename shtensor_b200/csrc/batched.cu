@@ -492,6 +492,11 @@ long long batched_multi_launch(sht_ctx* ctx, const std::vector<sht_plan*>& plans
   return total;
 }
 
+void batched_launch(sht_plan* p, const SparseArgs& g, cudaStream_t s) {
+  BatchedArgs b = batched_args(p, g);
+  launch_batched(p, b, s);
+}
+
 void batched_execute(sht_plan* p, const SparseArgs& g, long long, cudaStream_t s) {
   BatchedArgs b = batched_args(p, g);
   if (!g.sc.alpha_zero) matform_execute(p, g.sc.alpha, s);

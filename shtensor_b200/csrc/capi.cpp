@@ -72,6 +72,35 @@ static void contract_split(sht_plan* p, double alpha, double beta, cudaStream_t 
   trace("contract: checked", s);
 }
 
+// Batched form of sht_contract, overlapped the same way: the matrix form of A and B (patterns
+// and values of A and B only) on the caller's stream, the plan and its size-class work list on
+// the lane stream.
+static void contract_batched(sht_plan* p, double alpha, double beta, cudaStream_t s) {
+  sht_ctx* ctx = p->ctx;
+  LaneLease lane(ctx);
+  const cudaStream_t ps = lane.lane.stream;
+  SHT_CUDA(cudaEventRecord(lane.lane.start, s));
+  p->d_counter = PoolBuf(ctx->pool.get(), 256, s);
+  matform_prepare(p, s);
+  uint64_t ab;
+  std::memcpy(&ab, &alpha, 8);
+  if (ab != 0) matform_execute(p, alpha, s);
+  trace("contract: matrix form launched", s);
+  SHT_CUDA(cudaStreamWaitEvent(ps, lane.lane.start, 0));
+  try {
+    plan_build(p, ps, true);
+    device_work_list(p, 0, 0, true, ps);
+  } catch (const PatternGrew&) {
+    plan_build(p, ps, false);
+    device_work_list(p, 0, 0, true, ps);
+  }
+  SHT_CUDA(cudaEventRecord(lane.lane.done, ps));
+  SHT_CUDA(cudaStreamWaitEvent(s, lane.lane.done, 0));
+  plan_touch(p, s);
+  batched_launch(p, sparse_args(p, alpha, beta), s);
+  trace("contract: batched kernel launched", s);
+}
+
 static void prepare_mode(sht_plan* p, cudaStream_t s) {
   if (p->mode == SHT_MODE_BATCHED_FP64) batched_prepare(p, s);
   if (p->mode == SHT_MODE_SPLIT) split_prepare(p, p->ctx->split_slices ? p->ctx->split_slices : split_slices_default(), s);
@@ -504,6 +533,9 @@ sht_status sht_contract(sht_ctx* ctx, const char* expr, double alpha, sht_tensor
     if (mode == SHT_MODE_SPLIT) {
       p.reset(plan_init(ctx, expr, A, B, C, eps, norm, mode, s));
       contract_split(p.get(), alpha, beta, s);
+    } else if (mode == SHT_MODE_BATCHED_FP64) {
+      p.reset(plan_init(ctx, expr, A, B, C, eps, norm, mode, s));
+      contract_batched(p.get(), alpha, beta, s);
     } else {
       p.reset(plan_create(ctx, expr, A, B, C, eps, norm, mode, s));
       prepare_mode(p.get(), s);

@@ -90,6 +90,8 @@ void device_work_list(sht_plan* p, int fixed_tm, int fixed_tn, bool per_class, c
                       const DevSum* extra = nullptr, long long* extra_out = nullptr, int nextra = 0);
 void plan_execute(sht_plan* p, double alpha, double beta, cudaStream_t s);
 void batched_prepare(sht_plan* p, cudaStream_t s);
+// the persistent kernel alone, with the operands already in matrix form (matform_execute)
+void batched_launch(sht_plan* p, const SparseArgs& g, cudaStream_t s);
 void batched_execute(sht_plan* p, const SparseArgs& g, long long nwork_plain, cudaStream_t s);
 void autotune(sht_plan* p, const char* cache_file, cudaStream_t s);
 void matform_prepare(sht_plan* p, cudaStream_t s);

@@ -81,19 +81,20 @@ __global__ void __launch_bounds__(256) k_matform(const double* __restrict__ src,
 // Items: slabs of about kSlabElems matrix-form elements (whole blocks when smaller).
 constexpr long long kSlabElems = 1 << 15;
 
-static void layout(const sht_tensor* T, const std::vector<int>& free_modes, const std::vector<int>& k_modes,
+static void layout(sht_tensor* T, const std::vector<int>& free_modes, const std::vector<int>& k_modes,
                    std::vector<long long>& off, std::vector<int>& ld, std::vector<int>& k4, long long& total,
                    std::vector<int4>& items) {
   const long long n = T->nblocks;
+  const int* dims = tensor_host_dims(T);
   off.resize(n);
   ld.resize(n);
   k4.resize(n);
   total = 0;
   for (long long b = 0; b < n; ++b) {
-    const int64_t id = T->ids[b];
+    const int* d = dims + b * T->order;
     long long m = 1, K = 1;
-    for (int ax : free_modes) m *= T->bs[ax][(id / T->gstride[ax]) % T->nblk[ax]];
-    for (int ax : k_modes) K *= T->bs[ax][(id / T->gstride[ax]) % T->nblk[ax]];
+    for (int ax : free_modes) m *= d[ax];
+    for (int ax : k_modes) K *= d[ax];
     const long long L = (m + 1) & ~1LL, K4 = (K + 3) & ~3LL;
     if (L * K4 >= (1LL << 31)) fail(SHT_ERR_UNSUPPORTED, "matrix form of a block above 2^31 elements");
     off[b] = total;
@@ -139,7 +140,7 @@ void matform_prepare(sht_plan* p, cudaStream_t s) {
     SHT_CUDA(cudaMemcpyAsync(p->mf_boff.ptr, ob.data(), nB * 8, cudaMemcpyHostToDevice, s));
     SHT_CUDA(cudaMemcpyAsync(p->mf_bld.ptr, lb.data(), nB * 4, cudaMemcpyHostToDevice, s));
   }
-  SHT_CUDA(cudaStreamSynchronize(s));  // host vectors are pageable
+  // (copies from pageable memory have consumed their source when they return)
   p->mf_elems = ta + tb;
 }
 
