@@ -235,6 +235,12 @@ __device__ __forceinline__ double i2d(long long x) {
   return __longlong_as_double(0x4338000000000000LL + x) - 6755399441055744.0;
 }
 
+// int32 -> double exactly: the double with high word 0x43300000 and low word x + 2^31 (as
+// unsigned) is 2^52 + x + 2^31; one integer operation and one FP64 add
+__device__ __forceinline__ double i32_to_d(int x) {
+  return __hiloint2double(0x43300000, x ^ (int)0x80000000) - 4503601774854144.0;
+}
+
 // 2^k as a double for -1022 <= k <= 1023 (exact)
 __device__ __forceinline__ double pow2(int k) { return __longlong_as_double((long long)(k + 1023) << 52); }
 
@@ -398,8 +404,10 @@ __device__ __forceinline__ bool split_wait(void* mbar, unsigned parity, volatile
 }
 
 // S (slices per operand) is a template parameter so that the group loops of the MMA issuer
-// and of the reassembly unroll completely; one instance per S = 1..8.
-template <int S>
+// and of the reassembly unroll completely; one instance per S = 1..8.  Narrow: every group sum
+// is below 2^23 in magnitude (the host checks S * 127^2 * K), so two groups combine exactly in
+// 32 bits and convert with one integer operation and one FP64 add.
+template <int S, bool Narrow>
 __global__ void __launch_bounds__(kSplitThreads, 1) k_split(SplitArgs g) {
   extern __shared__ __align__(1024) unsigned char smem_raw[];
   SplitSmem& sm = *reinterpret_cast<SplitSmem*>(smem_raw);
@@ -603,12 +611,31 @@ __global__ void __launch_bounds__(kSplitThreads, 1) k_split(SplitArgs g) {
             }
             // the triple's lowest group has weight 2^(-7(g0 + len - 1)) relative to group 2
             const double w = pow2(-7 * (g0 + len - 1));
+            if constexpr (Narrow) {
+              // P_g 2^7 + P_{g+1} < 2^31: the first two groups of the triple in 32 bits, the
+              // third on its own (smallest weight first)
 #pragma unroll
-            for (int j = 0; j < 8; ++j) {
-              long long x = (int)v[0][j];
-              if (len > 1) x = x * 128 + (int)v[1][j];
-              if (len > 2) x = x * 128 + (int)v[2][j];
-              part[j] = fma(i2d(x), w, part[j]);
+              for (int j = 0; j < 8; ++j) {
+                if (len == 1) {
+                  part[j] = fma(i32_to_d((int)v[0][j]), w, part[j]);
+                } else {
+                  const int x01 = (int)v[0][j] * 128 + (int)v[1][j];
+                  if (len == 2) {
+                    part[j] = fma(i32_to_d(x01), w, part[j]);
+                  } else {
+                    part[j] = fma(i32_to_d((int)v[2][j]), w, part[j]);
+                    part[j] = fma(i32_to_d(x01), w * 128.0, part[j]);
+                  }
+                }
+              }
+            } else {
+#pragma unroll
+              for (int j = 0; j < 8; ++j) {
+                long long x = (int)v[0][j];
+                if (len > 1) x = x * 128 + (int)v[1][j];
+                if (len > 2) x = x * 128 + (int)v[2][j];
+                part[j] = fma(i2d(x), w, part[j]);
+              }
             }
           }
         }
@@ -789,18 +816,35 @@ constexpr size_t kSplitSmemLaunch = sizeof(SplitSmem);
 static_assert(kSplitSmemLaunch > 114 * 1024, "one split CTA per SM");
 
 using SplitKernel = void (*)(SplitArgs);
-static const SplitKernel kSplitKernels[kMaxSlices] = {k_split<1>, k_split<2>, k_split<3>, k_split<4>,
-                                                      k_split<5>, k_split<6>, k_split<7>, k_split<8>};
+static const SplitKernel kSplitKernels[2][kMaxSlices] = {
+    {k_split<1, false>, k_split<2, false>, k_split<3, false>, k_split<4, false>, k_split<5, false>,
+     k_split<6, false>, k_split<7, false>, k_split<8, false>},
+    {k_split<1, true>, k_split<2, true>, k_split<3, true>, k_split<4, true>, k_split<5, true>, k_split<6, true>,
+     k_split<7, true>, k_split<8, true>}};
+
+// every group sum below 2^23: S * 127^2 * K for the largest padded contracted extent K (the
+// product of the largest block extents of the contracted modes)
+static bool split_narrow(const sht_plan* p, int S) {
+  long double kmax = 1;
+  for (int ax : p->maps.colA) {
+    int mx = 0;
+    for (int v : p->A->bs[ax]) mx = std::max(mx, v);
+    kmax *= mx;
+  }
+  const long double kp = std::ceil(kmax / kSplitK) * kSplitK;
+  return (long double)S * 16129.0L * kp < 8388608.0L;
+}
 
 static int split_grid(sht_ctx* ctx) {
   static std::once_flag once;
   std::call_once(once, [] {
-    for (SplitKernel k : kSplitKernels) {
-      SHT_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSplitSmemLaunch));
-      int n = 0;
-      SHT_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k, kSplitThreads, kSplitSmemLaunch));
-      if (n != 1) fail(SHT_ERR_STATE, "split kernel must run one CTA per SM (TMEM budget)");
-    }
+    for (const auto& row : kSplitKernels)
+      for (SplitKernel k : row) {
+        SHT_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSplitSmemLaunch));
+        int n = 0;
+        SHT_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k, kSplitThreads, kSplitSmemLaunch));
+        if (n != 1) fail(SHT_ERR_STATE, "split kernel must run one CTA per SM (TMEM budget)");
+      }
   });
   return ctx->num_sms;
 }
@@ -857,7 +901,7 @@ void split_launch(sht_plan* p, const SparseArgs& sa, cudaStream_t s) {
   g.wait_limit = 1LL << 22;
   if (g.nwork <= 0) return;
   const int grid = (int)std::min<long long>(split_grid(p->ctx), g.nwork);
-  kSplitKernels[S - 1]<<<grid, kSplitThreads, kSplitSmemLaunch, s>>>(g);
+  kSplitKernels[split_narrow(p, S) ? 1 : 0][S - 1]<<<grid, kSplitThreads, kSplitSmemLaunch, s>>>(g);
   SHT_CUDA(cudaGetLastError());
 }
 
