@@ -1,6 +1,6 @@
-// peaks.cu -- in-run roofline denominators that the pool's measured-peaks file lacks.
+// peaks.cu -- in-run roofline denominators that the measured-peaks file (HBM copy, bf16 GEMM) lacks.
 //   which = 0: FP64 FMA throughput (TFLOP/s) from independent DFMA chains on every SM.
-// The contraction's FP64 tile kernel is judged against this figure.
+// The contraction's FP64 tile kernel is measured against this figure.
 #include "sht_internal.h"
 
 namespace sht {
