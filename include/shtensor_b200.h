@@ -21,6 +21,7 @@
  *   sht_kernel_info              KernelBase::get_info()                 src/Kernel/Kernel.cpp:29-32
  *   sht_tensor_create            Tensor<T,N>(ctx, VArray<N> block_sizes) src/Tensor/Tensor.h:27-32
  *   sht_tensor_reserve(_all)     BaseTensor::reserve / reserve_all      src/Tensor/BaseTensor.cpp:97-251
+ *   sht_tensor_reserve_device    BaseTensor::reserve, index lists on the device  BaseTensor.cpp:117-251
  *   sht_tensor_get_index         BaseTensor::get_sparse_info()          src/Tensor/BaseTensor.h:51
  *   sht_tensor_upload/download   block data access (get_local_block, iterators)
  *                                                                       src/Tensor/Tensor.h:38-52,75-258
@@ -125,6 +126,11 @@ sht_status sht_tensor_create(sht_ctx* ctx, int order, const int* nblk, const int
                              sht_dtype dtype, sht_tensor** out);
 /* idx is mode-major like VArray<N>: idx[d*nblocks + b]; zero-fills the data */
 sht_status sht_tensor_reserve(sht_tensor* t, int64_t nblocks, const int* idx);
+/* The same as sht_tensor_reserve (BaseTensor::reserve, src/Tensor/BaseTensor.cpp:117-251) with
+ * the index lists already in device memory (idx[d * nblocks + b], int32): the ids, their sort,
+ * the range / duplicate / size checks and the offsets are built on the GPU, with one read-back
+ * of the checks and the element count; blocks start zero-filled.  Returns after the build. */
+sht_status sht_tensor_reserve_device(sht_tensor* t, int64_t nblocks, const int* idx, void* stream);
 sht_status sht_tensor_reserve_all(sht_tensor* t);
 sht_status sht_tensor_info(const sht_tensor* t, int64_t* nblocks, int64_t* nnz);
 /* host copies of the sparse index: sorted rolled ids, element offsets, rows (nblk[0]) */

@@ -113,6 +113,7 @@ _SIGS = {
     "sht_tensor_create": [_P, C.c_int, _P, _P, C.c_int, C.POINTER(_P)],
     "sht_tensor_reserve": [_P, C.c_int64, _P],
     "sht_tensor_reserve_all": [_P],
+    "sht_tensor_reserve_device": [_P, C.c_int64, _P, _P],
     "sht_tensor_info": [_P, C.POINTER(C.c_int64), C.POINTER(C.c_int64)],
     "sht_tensor_get_index": [_P, _P, _P, _P],
     "sht_tensor_upload": [_P, _P, C.c_int64, _P],
@@ -321,6 +322,23 @@ class Tensor:
         flat = np.ascontiguousarray(np.concatenate([np.asarray(v, dtype=np.int32) for v in idx])) if n else \
             np.zeros(1, np.int32)
         _check(lib().sht_tensor_reserve(self._h, C.c_int64(n), flat.ctypes.data_as(_P)))
+        return self
+
+    def reserve_device(self, idx, nblocks=None, stream=None):
+        """Reserve from index lists in device memory: idx is a CUDA int32 tensor of shape
+        (order, nblocks) (mode-major, like reserve's lists), or a raw device pointer with
+        nblocks given."""
+        if hasattr(idx, "data_ptr"):
+            if idx.dtype != __import__("torch").int32 or not idx.is_cuda or idx.dim() != 2 \
+                    or idx.shape[0] != self.order:
+                raise ValueError("reserve_device: a CUDA int32 tensor of shape (order, nblocks)")
+            idx = idx.contiguous()
+            nblocks = idx.shape[1]
+            ptr = idx.data_ptr()
+        else:
+            ptr = int(idx)
+        _check(lib().sht_tensor_reserve_device(self._h, C.c_int64(int(nblocks)), C.c_void_p(ptr or None),
+                                               _stream(stream)))
         return self
 
     def reserve_all(self):

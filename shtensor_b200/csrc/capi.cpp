@@ -332,6 +332,13 @@ sht_status sht_tensor_reserve(sht_tensor* t, int64_t nblocks, const int* idx) {
   });
 }
 
+sht_status sht_tensor_reserve_device(sht_tensor* t, int64_t nblocks, const int* idx, void* stream) {
+  return guard([&] {
+    need(t, "null tensor");
+    tensor_reserve_device(t, nblocks, idx, as_stream(stream));
+  });
+}
+
 sht_status sht_tensor_reserve_all(sht_tensor* t) {
   return guard([&] {
     need(t, "null tensor");

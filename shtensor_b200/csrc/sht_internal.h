@@ -227,6 +227,8 @@ void parse_einsum(const std::string& expr, int nA, const int* sA, int nB, const 
 
 // tensors (tensor.cu)
 void tensor_set_index(sht_tensor* t, std::vector<int64_t>&& ids, cudaStream_t s);
+// reserve from mode-major index lists in device memory (ids, sort, checks and offsets on the GPU)
+void tensor_reserve_device(sht_tensor* t, long long n, const int* d_idx, cudaStream_t s);
 void tensor_sync_host(sht_tensor* t, cudaStream_t s);
 // per-block extents of the host index, nblocks x order (the host index must be current)
 const int* tensor_host_dims(sht_tensor* t);

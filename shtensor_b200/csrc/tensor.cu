@@ -126,6 +126,94 @@ const int* tensor_host_coords(sht_tensor* t) {
   return t->hcoords.data();
 }
 
+// ---------------------------------------------------------------------------------------
+// reserve from index lists already on the device (BaseTensor::reserve, BaseTensor.cpp:117-251,
+// with the ids, their sort and the offsets built on the GPU)
+// ---------------------------------------------------------------------------------------
+// idx is mode-major (idx[d * n + b]) like sht_tensor_reserve's host lists.  Bad entries set bit 0
+// of *bad and give id 0 (the build is then abandoned).
+__global__ void k_ids_from_lists(TensorMeta m, const int* __restrict__ idx, long long n, long long* __restrict__ ids,
+                                 int* __restrict__ bad) {
+  for (long long b = blockIdx.x * (long long)blockDim.x + threadIdx.x; b < n; b += (long long)gridDim.x * blockDim.x) {
+    long long id = 0;
+    bool ok = true;
+    for (int d = 0; d < m.order; ++d) {
+      const int v = idx[(long long)d * n + b];
+      if (v < 0 || v >= m.nblk[d]) ok = false;
+      else id += (long long)v * m.gstride[d];
+    }
+    if (!ok) {
+      atomicOr(bad, 1);
+      id = 0;
+    }
+    ids[b] = id;
+  }
+}
+
+// On the sorted ids: bit 1 for a repeated id, bit 2 for a block of 2^31 elements or more; the
+// last thread also leaves the element count (offset + size of the last block) in *nnz.
+__global__ void k_reserve_checks(const long long* __restrict__ ids, const long long* __restrict__ sizes,
+                                 const long long* __restrict__ offs, long long n, int* __restrict__ bad,
+                                 long long* __restrict__ nnz) {
+  for (long long b = blockIdx.x * (long long)blockDim.x + threadIdx.x; b < n; b += (long long)gridDim.x * blockDim.x) {
+    if (b > 0 && ids[b] == ids[b - 1]) atomicOr(bad, 2);
+    if (sizes[b] >= (1LL << 31)) atomicOr(bad, 4);
+    if (b == n - 1) *nnz = offs[b] + sizes[b];
+  }
+}
+
+void tensor_reserve_device(sht_tensor* t, long long n, const int* d_idx, cudaStream_t s) {
+  if (n < 0 || (n > 0 && !d_idx)) fail(SHT_ERR_INVALID, "bad index list");
+  if (n > (long long)INT32_MAX) fail(SHT_ERR_UNSUPPORTED, "reserve: more than 2^31 blocks");
+  DevicePool* pool = t->ctx->pool.get();
+  tensor_touch(t, s);
+  const long long nn = std::max(n, 1LL);
+  PoolBuf ids(pool, nn * 8, s), sorted(pool, nn * 8, s), dims(pool, nn * t->order * 4, s), sizes(pool, nn * 8, s),
+      offs(pool, nn * 8, s), word(pool, 16, s);
+  SHT_CUDA(cudaMemsetAsync(word.ptr, 0, 16, s));
+  const TensorMeta m = make_meta(t);
+  if (n > 0) {
+    k_ids_from_lists<<<grid_for(n, 256), 256, 0, s>>>(m, d_idx, n, ids.as<long long>(), word.as<int>());
+    SHT_CUDA(cudaGetLastError());
+    long double grid = 1;
+    for (int d = 0; d < t->order; ++d) grid *= t->nblk[d];
+    int bits = 1;
+    while (bits < 63 && (long double)(1ULL << bits) < grid) ++bits;
+    size_t tb = 0;
+    cub::DeviceRadixSort::SortKeys(nullptr, tb, ids.as<long long>(), sorted.as<long long>(), (int)n, 0, bits, s);
+    {
+      PoolBuf tmp(pool, tb, s);
+      cub::DeviceRadixSort::SortKeys(tmp.ptr, tb, ids.as<long long>(), sorted.as<long long>(), (int)n, 0, bits, s);
+    }
+    k_block_dims<<<grid_for(n, 256), 256, 0, s>>>(m, sorted.as<long long>(), n, dims.as<int>(), sizes.as<long long>());
+    SHT_CUDA(cudaGetLastError());
+    cub::DeviceScan::ExclusiveSum(nullptr, tb, sizes.as<long long>(), offs.as<long long>(), (int)n, s);
+    {
+      PoolBuf tmp(pool, tb, s);
+      cub::DeviceScan::ExclusiveSum(tmp.ptr, tb, sizes.as<long long>(), offs.as<long long>(), (int)n, s);
+    }
+    k_reserve_checks<<<grid_for(n, 256), 256, 0, s>>>(sorted.as<long long>(), sizes.as<long long>(),
+                                                      offs.as<long long>(), n, word.as<int>(),
+                                                      word.as<long long>() + 1);
+    SHT_CUDA(cudaGetLastError());
+  }
+  long long h[2] = {0, 0};
+  SHT_CUDA(cudaMemcpyAsync(h, word.ptr, 16, cudaMemcpyDeviceToHost, s));  // pageable: returns when done
+  const int bad = (int)(h[0] & 0xffffffff);
+  if (bad & 1) fail(SHT_ERR_INVALID, "reserve: block index out of range");
+  if (bad & 2) fail(SHT_ERR_INVALID, "reserve: duplicate block index");
+  if (bad & 4) fail(SHT_ERR_UNSUPPORTED, "block above 2^31 elements");
+  const long long nnz = h[1];
+  t->d_ids = std::move(sorted);
+  t->d_offsets = std::move(offs);
+  t->d_dims = std::move(dims);
+  t->d_data = PoolBuf(pool, std::max(nnz, 1LL) * t->esize(), s);
+  SHT_CUDA(cudaMemsetAsync(t->d_data.ptr, 0, std::max(nnz, 1LL) * t->esize(), s));
+  t->nblocks = n;
+  t->nnz = nnz;
+  t->host_stale = true;  // the host mirror is read back when a host-side step needs it
+}
+
 void tensor_touch(sht_tensor* t, cudaStream_t s) {
   for (PoolBuf* b : {&t->d_bsizes, &t->d_bstart, &t->d_ids, &t->d_offsets, &t->d_dims, &t->d_data}) b->use_on(s);
 }

@@ -36,6 +36,50 @@ def test_reserve_index_lists_and_errors(ctx):
         sht.Tensor(ctx, [[2, 3]])  # order < 2
 
 
+def test_reserve_device_matches_host_reserve(ctx):
+    # index lists in device memory, in no particular order: the same sorted ids, offsets and
+    # rows as the host reserve and as the oracle's restatement; then used as a contraction
+    # operand, the same result bits as the host-reserved tensor
+    import torch
+    w = W.c0(seed=12, nblocks=10, p=0.35)
+    rng = np.random.default_rng(13)
+    lists = w.A.index_lists()
+    perm = rng.permutation(len(w.A.ids))
+    idx = np.stack([np.asarray(v, np.int32)[perm] for v in lists])
+    Ah = sht.Tensor(ctx, w.A.block_sizes).reserve(lists)
+    Ad = sht.Tensor(ctx, w.A.block_sizes).reserve_device(torch.from_numpy(idx).cuda())
+    want = oracle.reserve(w.A.block_sizes, [list(v) for v in lists])
+    for t in (Ah, Ad):
+        ids, offs, rows = t.get_sparse_info()
+        assert np.array_equal(ids, want.ids) and np.array_equal(offs, want.offsets) and np.array_equal(rows, want.rows)
+    assert Ad.info() == Ah.info()
+    assert not Ad.download().any()
+    Ah.upload(w.A.data)
+    Ad.upload(w.A.data)
+    B = sht.Tensor(ctx, w.B.block_sizes).reserve(w.B.index_lists())
+    B.upload(w.B.data)
+    Ch, Cd = sht.Tensor(ctx, w.C.block_sizes), sht.Tensor(ctx, w.C.block_sizes)
+    sht.contract(ctx, w.expr, 1.0, Ah, B, 0.0, Ch, mode=sht.Mode.PLAIN_FP64)
+    sht.contract(ctx, w.expr, 1.0, Ad, B, 0.0, Cd, mode=sht.Mode.PLAIN_FP64)
+    assert np.array_equal(Ch.get_sparse_info()[0], Cd.get_sparse_info()[0])
+    assert np.array_equal(Ch.download().view(np.uint64), Cd.download().view(np.uint64))
+
+
+def test_reserve_device_errors_and_empty(ctx):
+    import torch
+    bs = BS4[:3]
+    dup = torch.tensor([[0, 1, 0], [1, 2, 1], [2, 0, 2]], dtype=torch.int32, device="cuda")
+    with pytest.raises(sht.ShtError) as ei:
+        sht.Tensor(ctx, bs).reserve_device(dup)
+    assert ei.value.status == sht.Status.ERR_INVALID
+    out = torch.tensor([[0, 4], [1, 1], [2, 6]], dtype=torch.int32, device="cuda")  # 4 and 6 are past the grid
+    with pytest.raises(sht.ShtError) as ei:
+        sht.Tensor(ctx, bs).reserve_device(out)
+    assert ei.value.status == sht.Status.ERR_INVALID
+    t = sht.Tensor(ctx, bs).reserve_device(torch.zeros((3, 0), dtype=torch.int32, device="cuda"))
+    assert t.info() == (0, 0)
+
+
 @pytest.mark.parametrize("norm", [sht.BlockNorm.FROBENIUS, sht.BlockNorm.MAXABS, sht.BlockNorm.FROBENIUS_REFCOMPAT])
 def test_norms_bit_exact(ctx, norm):
     w = W.c0(seed=2, nblocks=6, p=0.5)
