@@ -120,6 +120,11 @@ class Tensor {
     detail::check(sht_tensor_reserve(t_, (int64_t)n, flat.data()));
   }
   void reserve(const VArray<N>& idx) { reserve(idx.data()); }
+  // index lists already in device memory, mode-major (d_idx[d * nblocks + b]); see
+  // sht_tensor_reserve_device
+  void reserve_device(const int* d_idx, int64_t nblocks, void* stream = nullptr) {
+    detail::check(sht_tensor_reserve_device(t_, nblocks, d_idx, stream));
+  }
 
   int64_t get_nb_nzblocks_local() const {
     int64_t nb = 0, nnz = 0;
