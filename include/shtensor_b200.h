@@ -112,8 +112,9 @@ sht_status sht_kernel_call(sht_kernel* k, const void* a, const void* b, void* c,
  * bits equal sht_kernel_call's.  Its only scratch is a static 32 MiB device array that every
  * GPU loading the library keeps until exit: a stack needing more (nb_ops * (m_pad + n_pad) *
  * K4 * 8 bytes, m_pad/n_pad rounded up to even, K4 to a multiple of 4) is rejected with
- * SHT_ERR_SIZE.  The first call on a device looks the array up (cudaGetSymbolAddress) and
- * should come before any stream capture.  Calls share the array: calls that overlap on the
+ * SHT_ERR_SIZE.  The first call on a device looks the array up (cudaGetSymbolAddress) and,
+ * under lazy module loading, loads the module (committing the array): it should come before
+ * any stream capture.  Calls share the array: calls that overlap on the
  * GPU race. */
 sht_status sht_kernel_call_static(sht_kernel* k, const double* a, const double* b, double* c, int64_t nb_ops,
                                   void* stream);
@@ -129,7 +130,8 @@ sht_status sht_tensor_reserve(sht_tensor* t, int64_t nblocks, const int* idx);
 /* The same as sht_tensor_reserve (BaseTensor::reserve, src/Tensor/BaseTensor.cpp:117-251) with
  * the index lists already in device memory (idx[d * nblocks + b], int32): the ids, their sort,
  * the range / duplicate / size checks and the offsets are built on the GPU, with one read-back
- * of the checks and the element count; blocks start zero-filled.  Returns after the build. */
+ * of the checks and the element count; blocks start zero-filled.  Returns after the build and
+ * the zero fill are done. */
 sht_status sht_tensor_reserve_device(sht_tensor* t, int64_t nblocks, const int* idx, void* stream);
 sht_status sht_tensor_reserve_all(sht_tensor* t);
 sht_status sht_tensor_info(const sht_tensor* t, int64_t* nblocks, int64_t* nnz);

@@ -10,8 +10,9 @@
 // exits.
 //
 // Set-up: the first call on a device (with that device current) looks up the array's device
-// address with cudaGetSymbolAddress and caches it; make that first call outside any stream
-// capture.  All calls share the one array and it keeps the last call's contents: every call
+// address with cudaGetSymbolAddress and caches it.  Under CUDA's lazy module loading that
+// first call is also the one that loads this library's module on the device, which commits
+// the 32 MiB array; make that first call outside any stream capture.  All calls share the one array and it keeps the last call's contents: every call
 // rewrites the part it uses (padding included) before reading it, and calls whose work
 // overlaps on the GPU (other streams, or another thread) race on it.
 #include <cstring>
@@ -95,6 +96,9 @@ __global__ void __launch_bounds__(256) k_matform_stack(const double* __restrict_
 }
 
 using StaticCfg = PipeCfg<64, 64, 2>;
+// launched with the default dynamic shared-memory limit on every device: no per-device
+// cudaFuncSetAttribute is needed
+static_assert(sizeof(PipeSmem<StaticCfg>) <= 48 * 1024, "static stack tile must fit the default 48 KB");
 
 struct StackTiles {
   TileMaps mp;
@@ -202,12 +206,6 @@ void stack_call_static(sht_kernel* k, const double* a, const double* b, double* 
   g.tiles_per_op = (int)(((m + StaticCfg::TM - 1) / StaticCfg::TM) * ((n + StaticCfg::TN - 1) / StaticCfg::TN));
   const long long blocks = nb_ops * g.tiles_per_op;
   if (blocks > 0x7fffffffLL) fail(SHT_ERR_UNSUPPORTED, "stack too large for one launch");
-  static bool attr = false;
-  if (!attr) {
-    SHT_CUDA(cudaFuncSetAttribute(k_stack_tc, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  (int)sizeof(PipeSmem<StaticCfg>)));
-    attr = true;
-  }
   k_stack_tc<<<(unsigned)blocks, 128, sizeof(PipeSmem<StaticCfg>), s>>>(g);
   SHT_CUDA(cudaGetLastError());
 }

@@ -209,6 +209,9 @@ void tensor_reserve_device(sht_tensor* t, long long n, const int* d_idx, cudaStr
   t->d_dims = std::move(dims);
   t->d_data = PoolBuf(pool, std::max(nnz, 1LL) * t->esize(), s);
   SHT_CUDA(cudaMemsetAsync(t->d_data.ptr, 0, std::max(nnz, 1LL) * t->esize(), s));
+  // the zero fill is done before the call returns, as for the host reserve: a later upload on
+  // another stream cannot be overtaken by it
+  SHT_CUDA(cudaStreamSynchronize(s));
   t->nblocks = n;
   t->nnz = nnz;
   t->host_stale = true;  // the host mirror is read back when a host-side step needs it

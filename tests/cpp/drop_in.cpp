@@ -1,9 +1,11 @@
 // C++ drop-in check: code written against shtensor's Kernel<T> / Tensor<T,N> API, compiled
 // against include/shtensor_b200.hpp and linked with libshtensor_b200.so.  Mirrors the
 // reference's own tests: test/test_kernel.cpp (test_contract, test_kernel's beta identity)
-// and test/test_tensor.cpp (360-block tensor, alternating-block filter + compress).
+// and test/test_tensor.cpp (360-block tensor walked with the block iterators, alternating-block
+// filter + compress through get_local_block).
 #include <cmath>
 #include <cstdio>
+#include <algorithm>
 #include <random>
 #include <vector>
 
@@ -73,6 +75,98 @@ static void test_tensor(Shtensor::Context& ctx) {
   for (float v : t.data()) CHECK(v == 1.f);
 }
 
+static void test_block_iteration(Shtensor::Context& ctx) {
+  // test/test_tensor.cpp:53-125: a 360-block tensor walked with the block iterators; every
+  // block filled through get_local_block with 0 or 1 by the parity of its id; filter without
+  // compress marks the zero blocks (negative ids), compress drops them
+  std::vector<int> dim0 = {4, 5, 3, 4}, dim1 = {5, 5, 8, 9, 2}, dim2 = {5, 6, 3, 7, 7, 9}, dim3 = {4, 3, 2};
+  Shtensor::VArray<4> bs4 = {dim0, dim1, dim2, dim3};
+  Shtensor::Tensor<float, 4> t(ctx, bs4);
+  t.reserve_all();
+  CHECK(t.get_nb_nzblocks_global() == 360);
+  int64_t nblocks = 0;
+  for (auto iter = t.begin(); iter != t.end(); ++iter) {
+    auto idx = iter.get_indices();
+    for (int d = 0; d < 4; ++d) CHECK(bs4[d][idx[d]] == iter->dim(d));
+    ++nblocks;
+  }
+  CHECK(nblocks == 360);
+  for (auto iter = t.begin(); iter != t.end(); ++iter) {
+    const int64_t iblk = iter - t.begin();
+    const int64_t blkid = iter.get_block_index();
+    auto block = t.get_local_block(iblk);
+    std::fill(block.begin(), block.end(), (blkid % 2 == 0) ? 0.f : 1.f);
+  }
+  t.filter(1e-6f, Shtensor::BlockNorm::FROBENIUS, false);
+  int64_t kept = 0;
+  for (auto iter = t.begin(); iter != t.end(); ++iter) {
+    const int64_t blkid = iter.get_block_index();
+    const int64_t ablkid = blkid >= 0 ? blkid : -(blkid + 1);
+    CHECK((ablkid % 2 == 0) == (blkid < 0));
+    kept += blkid < 0 ? 0 : 1;
+    // a marked block keeps its extents (indices of its original id)
+    auto idx = iter.get_indices();
+    for (int d = 0; d < 4; ++d) CHECK(bs4[d][idx[d]] == iter->dim(d));
+  }
+  t.compress();
+  for (auto iter = t.cbegin(); iter != t.cend(); ++iter) {
+    CHECK(iter.get_block_index() >= 0);
+    for (float v : *iter) CHECK(v == 1.f);
+  }
+  CHECK(kept == t.get_nb_nzblocks_local());
+  CHECK(kept == 180);
+}
+
+static void test_sparse_blocks_and_views(Shtensor::Context& ctx) {
+  // a sparse pattern: block sizes come from indices[b], not from the storage position
+  Shtensor::VArray<3> bs = {std::vector<int>{2, 3, 4}, std::vector<int>{5, 1}, std::vector<int>{3, 2, 6}};
+  Shtensor::Tensor<double, 3> t(ctx, bs);
+  const std::vector<int> i0 = {2, 0, 1, 2}, i1 = {1, 0, 1, 0}, i2 = {2, 1, 0, 0};
+  t.reserve(Shtensor::VArray<3>{i0, i1, i2});
+  auto info = t.get_sparse_info();
+  CHECK(info.indices.size() == 4);
+  // fill element (a, b, c) of every block with id * 1000 + a + 10 b + 100 c through operator()
+  for (int64_t b = 0; b < t.get_nb_nzblocks_local(); ++b) {
+    auto blk = t.get_local_block(b);
+    const auto idx = t.get_block_indices(b);
+    int64_t rolled = idx[0] + 3 * (idx[1] + 2 * idx[2]);
+    CHECK(rolled == info.indices[b]);
+    for (int d = 0; d < 3; ++d) CHECK(blk.dim(d) == bs[d][idx[d]]);
+    for (int c = 0; c < blk.dim(2); ++c)
+      for (int y = 0; y < blk.dim(1); ++y)
+        for (int a = 0; a < blk.dim(0); ++a) blk(a, y, c) = (double)(info.indices[b] * 1000 + a + 10 * y + 100 * c);
+  }
+  // data() writes the modified mirror back first; column-major layout within a block
+  const std::vector<double> all = t.data();
+  for (int64_t b = 0; b < (int64_t)info.indices.size(); ++b) {
+    auto blk = t.get_local_block(b);
+    for (int c = 0; c < blk.dim(2); ++c)
+      for (int y = 0; y < blk.dim(1); ++y)
+        for (int a = 0; a < blk.dim(0); ++a) {
+          const int64_t e = info.offsets[b] + a + blk.dim(0) * (y + blk.dim(1) * c);
+          CHECK(all[e] == (double)(info.indices[b] * 1000 + a + 10 * y + 100 * c));
+        }
+  }
+  // host norms of the views equal the device's, bit for bit (FROBENIUS and MAXABS)
+  for (auto norm : {Shtensor::BlockNorm::FROBENIUS, Shtensor::BlockNorm::MAXABS}) {
+    const auto dn = t.norms(norm);
+    int64_t b = 0;
+    for (auto it = t.cbegin(); it != t.cend(); ++it, ++b) CHECK(it->get_norm(norm) == dn[b]);
+  }
+  // random access
+  auto it = t.cbegin();
+  CHECK((it + 3)->dim(0) == bs[0][t.get_block_indices(3)[0]]);
+  CHECK(t.cend() - t.cbegin() == 4);
+  CHECK((it + 4) == t.cend() && (it + 4)->size() == 0);
+  // the device view points into the tensor's device data at the block's offset
+  auto dv = t.get_device_block(2);
+  auto hv = t.get_local_block(2);
+  CHECK(dv.size() == hv.size() && dv.dim(1) == hv.dim(1));
+  // an owning copy
+  Shtensor::Block<double, 3> copy(hv);
+  CHECK(copy.size() == hv.size() && copy(0, 0, 0) == hv(0, 0, 0) && copy.data() != hv.data());
+}
+
 static void test_blocksparse(Shtensor::Context& ctx) {
   // C[i,k] = sum_j A[i,j] B[j,k] over 3x3 block grids, all blocks present
   Shtensor::VArray<2> ba = {std::vector<int>{2, 3, 4}, std::vector<int>{3, 1, 2}};
@@ -98,6 +192,8 @@ int main() {
     test_contract<float>(ctx);
     test_beta(ctx);
     test_tensor(ctx);
+    test_block_iteration(ctx);
+    test_sparse_blocks_and_views(ctx);
     test_blocksparse(ctx);
   } catch (const std::exception& e) {
     std::printf("exception: %s\n", e.what());

@@ -35,3 +35,16 @@ def test_no_gpu_fails_loudly():
     with pytest.raises(sht.ShtError) as ei:
         sht.Context(1 << 20)
     assert ei.value.status in (sht.Status.ERR_CUDA, sht.Status.ERR_OOM)
+
+
+def test_cpp_drop_in_header_compiles(tmp_path):
+    # the C++ drop-in layer (Kernel<T>, Tensor<T,N> with get_local_block and the block
+    # iterators, BlockSpan) compiles and links against the library; it runs under -m gpu
+    import subprocess
+    exe = tmp_path / "drop_in"
+    libdir = os.path.dirname(sht.LIB_PATH)
+    cmd = ["g++", "-std=c++17", "-O1", "-Wall", "-Wextra", "-Werror", "-I", os.path.join(ROOT, "include"),
+           os.path.join(ROOT, "tests", "cpp", "drop_in.cpp"), "-L", libdir, "-lshtensor_b200",
+           f"-Wl,-rpath,{libdir}", "-o", str(exe)]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr

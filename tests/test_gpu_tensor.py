@@ -78,6 +78,27 @@ def test_reserve_device_errors_and_empty(ctx):
     assert ei.value.status == sht.Status.ERR_INVALID
     t = sht.Tensor(ctx, bs).reserve_device(torch.zeros((3, 0), dtype=torch.int32, device="cuda"))
     assert t.info() == (0, 0)
+    # one block of 2048 x 1024 x 1024 = 2^31 elements: rejected by the device-side size check
+    # before any data is allocated
+    big = sht.Tensor(ctx, [[2048, 3], [1024, 2], [1024]])
+    with pytest.raises(sht.ShtError) as ei:
+        big.reserve_device(torch.zeros((3, 1), dtype=torch.int32, device="cuda"))
+    assert ei.value.status == sht.Status.ERR_UNSUPPORTED
+    small = torch.tensor([[1], [1], [0]], dtype=torch.int32, device="cuda")  # a 3 x 2 x 1024 block
+    assert big.reserve_device(small).info() == (1, 3 * 2 * 1024)
+
+
+def test_reserve_device_on_side_stream_then_upload(ctx):
+    # reserve on a non-blocking stream, upload on the legacy default stream: the reserve's zero
+    # fill of the data must not land after the upload
+    import torch
+    w = W.c0(seed=21, nblocks=12, p=0.5)
+    idx = torch.from_numpy(np.stack([np.asarray(v, np.int32) for v in w.A.index_lists()])).cuda()
+    side = torch.cuda.Stream()
+    for _ in range(3):
+        t = sht.Tensor(ctx, w.A.block_sizes).reserve_device(idx, stream=side)
+        t.upload(w.A.data)
+        assert np.array_equal(t.download(), w.A.data)
 
 
 @pytest.mark.parametrize("norm", [sht.BlockNorm.FROBENIUS, sht.BlockNorm.MAXABS, sht.BlockNorm.FROBENIUS_REFCOMPAT])
