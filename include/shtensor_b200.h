@@ -165,6 +165,9 @@ sht_status sht_plan_destroy(sht_plan* p);
 /* ---- split-precision error report (max abs and relative Frobenius vs an FP64 result) ---- */
 sht_status sht_tensor_compare(sht_tensor* X, sht_tensor* Ref, double* max_abs, double* rel_fro,
                               void* stream);
+/* number of elements whose bit patterns differ between X and Ref (same block pattern): 0 means
+ * bit-identical results, signed zeros included (no reference counterpart; a parity check) */
+sht_status sht_tensor_bitdiff(sht_tensor* X, sht_tensor* Ref, int64_t* ndiff, void* stream);
 
 /* ---- autotuner ---- */
 /* sweeps tile shapes per (m,n,k) size class of the plan and stores the choice; file may be NULL */
@@ -175,7 +178,8 @@ sht_status sht_set_split_slices(sht_ctx* ctx, int slices);
 
 /* ---- diagnostics ---- */
 /* which = 0: FP64 FMA peak of this GPU in TFLOP/s (the FP64 kernels' roofline denominator);
- * which = 1: dense INT8 tensor-core (tcgen05 kind::i8) peak in TOPS (the split kernel's) */
+ * which = 1: dense INT8 tensor-core (tcgen05 kind::i8) peak in TOPS (the split kernel's);
+ * which = 2: FP64 tensor-core (mma.sync m8n8k4) peak in TFLOP/s (the batched kernel's) */
 sht_status sht_measure_peak(sht_ctx* ctx, int which, double* value);
 
 /* ---- serving loop (no reference counterpart: shtensor has no request loop) ----

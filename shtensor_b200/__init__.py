@@ -132,6 +132,7 @@ _SIGS = {
     "sht_plan_pairs": [_P, _P, C.c_int64],
     "sht_plan_destroy": [_P],
     "sht_tensor_compare": [_P, _P, C.POINTER(C.c_double), C.POINTER(C.c_double), _P],
+    "sht_tensor_bitdiff": [_P, _P, C.POINTER(C.c_int64), _P],
     "sht_autotune": [_P, C.c_char_p, _P],
     "sht_measure_peak": [_P, C.c_int, C.POINTER(C.c_double)],
     "sht_set_split_slices": [_P, C.c_int],
@@ -454,9 +455,9 @@ def contract(ctx: Context, expr: str, alpha: float, A: Tensor, B: Tensor, beta: 
 
 def measure_peak(ctx: Context, which: str = "fp64") -> float:
     """Roofline denominators measured on this GPU: 'fp64' = FP64 FMA TFLOP/s, 'int8' = dense
-    INT8 tensor-core TOPS."""
+    INT8 tensor-core TOPS, 'dmma' = FP64 tensor-core (m8n8k4) TFLOP/s."""
     v = C.c_double()
-    _check(lib().sht_measure_peak(ctx.handle, {"fp64": 0, "int8": 1}[which], C.byref(v)))
+    _check(lib().sht_measure_peak(ctx.handle, {"fp64": 0, "int8": 1, "dmma": 2}[which], C.byref(v)))
     return v.value
 
 
@@ -464,6 +465,13 @@ def compare(X: Tensor, Ref: Tensor, stream=None):
     mx, fr = C.c_double(), C.c_double()
     _check(lib().sht_tensor_compare(X.handle, Ref.handle, C.byref(mx), C.byref(fr), _stream(stream)))
     return mx.value, fr.value
+
+
+def bitdiff(X: Tensor, Ref: Tensor, stream=None) -> int:
+    """Number of elements whose bit patterns differ (0 = bit-identical, signed zeros included)."""
+    n = C.c_int64()
+    _check(lib().sht_tensor_bitdiff(X.handle, Ref.handle, C.byref(n), _stream(stream)))
+    return n.value
 
 
 class Server:

@@ -10,6 +10,7 @@ namespace sht {
 
 double measure_fp64_tflops(sht_ctx* ctx);
 double measure_int8_tops(sht_ctx* ctx);
+double measure_dmma_tflops(sht_ctx* ctx);
 void stack_call_static(sht_kernel* k, const double* a, const double* b, double* c, int64_t nb_ops, cudaStream_t s);
 
 // A lane (stream + two events) borrowed from the context for the length of one call.
@@ -565,7 +566,16 @@ sht_status sht_contract(sht_ctx* ctx, const char* expr, double alpha, sht_tensor
 sht_status sht_tensor_compare(sht_tensor* X, sht_tensor* Ref, double* max_abs, double* rel_fro, void* stream) {
   return guard([&] {
     need(X && Ref, "null tensor");
-    tensor_compare_device(X, Ref, max_abs, rel_fro, as_stream(stream));
+    tensor_compare_device(X, Ref, max_abs, rel_fro, nullptr, as_stream(stream));
+  });
+}
+
+sht_status sht_tensor_bitdiff(sht_tensor* X, sht_tensor* Ref, int64_t* ndiff, void* stream) {
+  return guard([&] {
+    need(X && Ref && ndiff, "null argument");
+    long long n = 0;
+    tensor_compare_device(X, Ref, nullptr, nullptr, &n, as_stream(stream));
+    *ndiff = n;
   });
 }
 
@@ -592,6 +602,8 @@ sht_status sht_measure_peak(sht_ctx* ctx, int which, double* value) {
       *value = measure_fp64_tflops(ctx);
     else if (which == 1)
       *value = measure_int8_tops(ctx);
+    else if (which == 2)
+      *value = measure_dmma_tflops(ctx);
     else
       fail(SHT_ERR_UNSUPPORTED, "unknown peak");
   });

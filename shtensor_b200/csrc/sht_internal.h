@@ -239,7 +239,8 @@ void tensor_norms_device(sht_tensor* t, sht_norm norm, double* d_out, cudaStream
 // is ordered after the work queued on `s` so far.
 void tensor_touch(sht_tensor* t, cudaStream_t s);
 int64_t block_size_of(const sht_tensor* t, int64_t id);
-void tensor_compare_device(sht_tensor* X, sht_tensor* R, double* max_abs, double* rel_fro, cudaStream_t s);
+void tensor_compare_device(sht_tensor* X, sht_tensor* R, double* max_abs, double* rel_fro, long long* ndiff,
+                           cudaStream_t s);
 
 // stack kernel (stack.cu)
 void stack_call(sht_kernel* k, const void* a, const void* b, void* c, int64_t nb_ops,

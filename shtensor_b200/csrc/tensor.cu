@@ -490,30 +490,38 @@ void tensor_filter_device(sht_tensor* t, double eps, sht_norm norm, int compress
 }
 
 // ---------------------------------------------------------------------------------------
-// Error of X against Ref over the same block pattern: max |x - r|, sum (x-r)^2, sum r^2.
+// Error of X against Ref over the same block pattern: max |x - r|, sum (x-r)^2, sum r^2, and the
+// number of elements whose bit patterns differ (signed zeros and NaN payloads count).
 // ---------------------------------------------------------------------------------------
 __global__ void k_compare(const double* __restrict__ x, const double* __restrict__ r, long long n,
-                          unsigned long long* __restrict__ maxbits, double* __restrict__ sums) {
+                          unsigned long long* __restrict__ maxbits, double* __restrict__ sums,
+                          unsigned long long* __restrict__ ndiff) {
   double mx = 0.0, d2 = 0.0, r2 = 0.0;
+  unsigned long long nd = 0;
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
-    const double d = x[i] - r[i];
+    const double xi = x[i], ri = r[i];
+    const double d = xi - ri;
     mx = fmax(mx, fabs(d));
     d2 = fma(d, d, d2);
-    r2 = fma(r[i], r[i], r2);
+    r2 = fma(ri, ri, r2);
+    nd += __double_as_longlong(xi) != __double_as_longlong(ri);
   }
   for (int off = 16; off >= 1; off >>= 1) {
     mx = fmax(mx, __shfl_down_sync(0xffffffffu, mx, off));
     d2 += __shfl_down_sync(0xffffffffu, d2, off);
     r2 += __shfl_down_sync(0xffffffffu, r2, off);
+    nd += __shfl_down_sync(0xffffffffu, nd, off);
   }
   if ((threadIdx.x & 31) == 0) {
     atomicMax(maxbits, (unsigned long long)__double_as_longlong(mx));  // non-negative: bit order = value order
     atomicAdd(&sums[0], d2);
     atomicAdd(&sums[1], r2);
+    atomicAdd(ndiff, nd);
   }
 }
 
-void tensor_compare_device(sht_tensor* X, sht_tensor* R, double* max_abs, double* rel_fro, cudaStream_t s) {
+void tensor_compare_device(sht_tensor* X, sht_tensor* R, double* max_abs, double* rel_fro, long long* ndiff,
+                           cudaStream_t s) {
   tensor_sync_host(X, s);
   tensor_sync_host(R, s);
   if (X->dtype != SHT_F64 || R->dtype != SHT_F64) fail(SHT_ERR_UNSUPPORTED, "compare runs on FP64 tensors");
@@ -522,15 +530,17 @@ void tensor_compare_device(sht_tensor* X, sht_tensor* R, double* max_abs, double
   SHT_CUDA(cudaMemsetAsync(acc.ptr, 0, 64, s));
   if (X->nnz)
     k_compare<<<grid_for(X->nnz, 256, X->ctx->num_sms * 8), 256, 0, s>>>(
-        X->d_data.as<double>(), R->d_data.as<double>(), X->nnz, acc.as<unsigned long long>(), acc.as<double>() + 1);
+        X->d_data.as<double>(), R->d_data.as<double>(), X->nnz, acc.as<unsigned long long>(), acc.as<double>() + 1,
+        acc.as<unsigned long long>() + 3);
   SHT_CUDA(cudaGetLastError());
-  double h[3];
-  SHT_CUDA(cudaMemcpyAsync(h, acc.ptr, 24, cudaMemcpyDeviceToHost, s));
+  double h[4];
+  SHT_CUDA(cudaMemcpyAsync(h, acc.ptr, 32, cudaMemcpyDeviceToHost, s));
   SHT_CUDA(cudaStreamSynchronize(s));
-  unsigned long long bits;
-  std::memcpy(&bits, &h[0], 8);
+  unsigned long long nd;
+  std::memcpy(&nd, &h[3], 8);
   if (max_abs) *max_abs = h[0];
   if (rel_fro) *rel_fro = h[2] > 0 ? std::sqrt(h[1] / h[2]) : std::sqrt(h[1]);
+  if (ndiff) *ndiff = (long long)nd;
 }
 
 }  // namespace sht

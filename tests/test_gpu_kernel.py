@@ -81,5 +81,7 @@ def test_measured_peaks_are_plausible(ctx):
     int8 = sht.measure_peak(ctx, "int8")
     assert 5.0 < fp64 < 200.0, fp64
     assert 100.0 < int8 < 20000.0, int8
+    dmma = sht.measure_peak(ctx, "dmma")
+    assert 5.0 < dmma < 200.0, dmma
     v = __import__("ctypes").c_double()
     assert sht.lib().sht_measure_peak(ctx.handle, 7, __import__("ctypes").byref(v)) == sht.Status.ERR_UNSUPPORTED
