@@ -1,11 +1,14 @@
 """Benchmark of the block-sparse contraction (one JSON line on rank 0).
 
-Workload: C[i,j,a,b] = sum_P A[i,a,P] B[j,b,P] at full size (i,j extent 64 in blocks of
-{5,9,13}; a,b 512 in {13,25,32}; P 2048 in {32,48,64}; 15% block occupancy; seeded values).
-A step is one full contraction C = A.B on the device: block matching, result pattern, work
-list and the tile kernel, inputs resident in HBM.  Metric: effective GFLOP/s =
-sum over pairs of 2*m*n*k / step time.  Every available FP64-accurate form is timed and the
-fastest is `value`; the others are listed under `forms`.
+Headline workload (``--workload c1``, the default): C[i,j,a,b] = sum_P A[i,a,P] B[j,b,P] at full
+size (i,j extent 64 in blocks of {5,9,13}; a,b 512 in {13,25,32}; P 2048 in {32,48,64}; 15%
+block occupancy; seeded values).  A step is one full contraction C = A.B on the device: block
+matching, result pattern, work list and the tile kernel, inputs resident in HBM.  Metric:
+effective GFLOP/s = sum over pairs of 2*m*n*k / step time.  Every FP64-accurate form is timed
+and the fastest is `value`; all are listed under `forms`, each checked against the CPU oracle
+on the full workload (pattern and pair list bit-exact, values bit-exact for the FP64 forms and
+within 1e-12 relative Frobenius for the split form).  The other configurations (c0, c2, c3)
+are timed and checked the same way under `configs`.
 
 `--impl reference` times the reference's CPU path of the same contraction (the LAPACK
 path of src/Kernel/KernelImpl.cpp:142-208 with the reference's own Utils::reshape, compiled
@@ -32,7 +35,14 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 METRIC = "block-sparse contract GFLOP/s (FP64-accurate)"
-WORKLOAD = "C[i,j,a,b]=sum_P A[i,a,P]*B[j,b,P]; i,j=64 in {5,9,13}; a,b=512 in {13,25,32}; P=2048 in {32,48,64}; occ 15%"
+WORKLOADS = {
+    "c0": "C[i,j,k]=sum_l A[i,j,l]*B[l,k]; 20 blocks per mode of U{5..15}; occ 0.3; U[-1,1] values",
+    "c1": "C[i,j,a,b]=sum_P A[i,a,P]*B[j,b,P]; i,j=64 in {5,9,13}; a,b=512 in {13,25,32}; P=2048 in {32,48,64}; occ 15%",
+    "c2": "c1 shapes with per-block magnitudes 10^U(-6,2)",
+    "c3": ("C[a,b,i,j]=sum_cd V[a,b,c,d]*T[c,d,i,j]; a..d extent 96 in blocks of 24-48, i,j 12 in 8-16 "
+           "(the configuration's extents x 1/8); V block kept iff exp(-0.5 spread) >= 0.1; product screening 1e-10"),
+}
+FORM_KERNEL = {"plain": "k_contract_tiles", "batched": "k_matform + k_batched", "split": "k_slice + k_split"}
 
 
 def parse():
@@ -41,22 +51,27 @@ def parse():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="c1", choices=sorted(WORKLOADS), help="the headline workload")
     ap.add_argument("--forms", default="plain,batched,split")
     ap.add_argument("--split-tol", type=float, default=1e-12,
-                    help="relative Frobenius error vs FP64 below which the split form counts as FP64-accurate")
-    ap.add_argument("--scale", type=float, default=1.0, help="extent scale of the workload (1.0 = full size)")
+                    help="relative Frobenius error vs the FP64 oracle below which the split form counts as FP64-accurate")
+    ap.add_argument("--scale", type=float, default=1.0, help="extent scale of the c0-c2 workloads (1.0 = full size)")
     ap.add_argument("--seed", type=int, default=1)
     ap.add_argument("--cpu-sample-seconds", type=float, default=15.0)
+    ap.add_argument("--cpu-runs", type=int, default=5, help="runs per CPU leg (the median is reported)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-count", action="store_true", help="skip the CUPTI launch count (use under ncu)")
     ap.add_argument("--no-autotune", action="store_true")
+    ap.add_argument("--no-oracle", action="store_true", help="skip the oracle checks (use under ncu)")
+    ap.add_argument("--no-configs", action="store_true", help="skip the other configurations")
     ap.add_argument("--pool-gb", type=float, default=60.0)
     ap.add_argument("--no-serving", action="store_true", help="skip the serving-loop phase")
     ap.add_argument("--serve-rate", type=float, default=200.0, help="Poisson arrival rate (requests/s)")
     ap.add_argument("--serve-seconds", type=float, default=2.0, help="length of the arrival stream")
     ap.add_argument("--serve-templates", type=int, default=16,
                     help="distinct requests (resident inputs) the stream draws from")
+    ap.add_argument("--serve-seeds", type=int, default=3, help="Poisson streams (seeds) of the serving phase")
     return ap.parse_args()
 
 
@@ -129,55 +144,84 @@ def replica_rate(work_per_rank: float, ms_per_rank: float, world: int) -> float:
     return world * work_per_rank / reduce_max(ms_per_rank) / 1e6
 
 
-def build_workload(args):
+def build_workload(name: str, seed: int = 1, scale: float = 1.0):
     from shtensor_b200 import workloads as W
-    return W.c1(seed=args.seed, scale=args.scale)
+    if name == "c0":
+        return W.c0(seed=seed)
+    if name == "c1":
+        return W.c1(seed=seed, scale=scale)
+    if name == "c2":
+        return W.c2(seed=seed, scale=scale)
+    return W.c3(seed=seed)
+
+
+def host(t):
+    import oracle
+    return oracle.HostTensor(t.block_sizes, t.ids, t.offsets, t.data)
+
+
+def pair_flops_per_a_block(w) -> np.ndarray:
+    """Algorithmic flops of each A block's pairs (no screening): 2 m_a k_a times the summed n
+    of the B blocks that share its contracted block indices."""
+    import oracle
+    mp = oracle.contract_info(w.expr, [1] * w.A.order, [1] * w.B.order, [1] * len(w.C.block_sizes))
+    ia, ib = w.A.index_lists(), w.B.index_lists()
+    da, db = w.A.block_dims(), w.B.block_dims()
+    ka = [tuple(int(ia[d][x]) for d in mp.colA) for x in range(len(w.A.ids))]
+    kb = [tuple(int(ib[d][x]) for d in mp.rowB) for x in range(len(w.B.ids))]
+    nb = db[:, mp.colB].prod(axis=1) if len(mp.colB) else np.ones(len(w.B.ids))
+    nsum: dict = {}
+    for key, n in zip(kb, nb):
+        nsum[key] = nsum.get(key, 0) + int(n)
+    m = da[:, mp.rowA].prod(axis=1).astype(np.float64)
+    k = da[:, mp.colA].prod(axis=1).astype(np.float64)
+    return np.array([2.0 * m[x] * k[x] * nsum.get(ka[x], 0) for x in range(len(w.A.ids))])
 
 
 def sample_workload(w, target_flops: float):
-    """Restrict A to its first i-blocks so that the sample's pair flops are about target."""
+    """The same contraction with A restricted to its blocks of mode-0 index below k, k chosen
+    so that the sample's pair flops reach about target (a bounded CPU sample)."""
     from shtensor_b200 import workloads as W
-    import oracle
-    H = lambda t: oracle.HostTensor(t.block_sizes, t.ids, t.offsets, t.data)  # noqa: E731
-    idx = w.A.index_lists()
-    dims = w.A.block_dims()
-    ni = len(w.A.block_sizes[0])
-    # flops per i-block, estimated from A block sizes x matching B volume per P block
-    Bidx = w.B.index_lists()
-    bvol = np.zeros(len(w.B.block_sizes[2]))
-    bd = w.B.block_dims()
-    np.add.at(bvol, Bidx[2], bd[:, 0] * bd[:, 1])
-    per_i = np.zeros(ni)
-    np.add.at(per_i, idx[0], 2.0 * dims[:, 0] * dims[:, 1] * dims[:, 2] * bvol[idx[2]])
+    idx0 = w.A.index_lists()[0]
+    fl = pair_flops_per_a_block(w)
+    n0 = len(w.A.block_sizes[0])
+    per0 = np.zeros(n0)
+    np.add.at(per0, idx0, fl)
     k = 1
-    while k < ni and per_i[:k].sum() < target_flops:
+    while k < n0 and per0[:k].sum() < target_flops:
         k += 1
-    keep = idx[0] < k
-    sizes = dims.prod(axis=1)
+    keep = idx0 < k
+    sizes = w.A.block_dims().prod(axis=1)
     offs = np.concatenate([[0], np.cumsum(sizes[keep])[:-1]]).astype(np.int64)
     data = np.concatenate([w.A.data[o:o + s] for o, s in zip(w.A.offsets[keep], sizes[keep])])
     A = W.HostBlockSparse(w.A.block_sizes, w.A.ids[keep], offs, data)
-    return W.Workload(w.name, w.expr, A, w.B, w.C), k, ni, H
+    return W.Workload(w.name, w.expr, A, w.B, w.C, screen_eps=w.screen_eps), k, n0
 
 
-def cpu_reference_run(w, seconds: float, nthreads: int):
-    """Time the reference CPU path on a sample sized to run about `seconds`."""
+def cpu_leg(w, seconds: float, nthreads: int, ref: bool, runs: int):
+    """Median rate (GFLOP/s) of `runs` runs of the CPU contraction on a sample sized to take about
+    `seconds` per run: ref=True is the reference's path (its own Utils::reshape + OpenBLAS dgemm
+    per pair, compiled from its sources into oracle/_ref), ref=False the oracle's bit-exact
+    XMM-order restatement.  OpenMP over C blocks with `nthreads` threads."""
     import oracle
-    H = lambda t: oracle.HostTensor(t.block_sizes, t.ids, t.offsets, t.data)  # noqa: E731
-    use_ref = oracle.ref_lib() is not None
-    kind = "reference" if use_ref else "port"
-    # calibrate on a small sample, then size the timed sample
-    probe, k, ni, _ = sample_workload(w, 2e9)
-    r = oracle.contract(probe.expr, 1.0, H(probe.A), H(probe.B), 0.0, H(probe.C), nthreads=nthreads, ref=use_ref,
-                        lapack_blocks=not use_ref)
+    probe, k, n0 = sample_workload(w, (0.5e9 if ref else 0.15e9) * max(nthreads, 1))
+    r = oracle.contract(probe.expr, 1.0, host(probe.A), host(probe.B), 0.0, host(probe.C), eps=probe.screen_eps,
+                        nthreads=nthreads, ref=ref)
     rate = r.flops / max(r.seconds, 1e-6)
-    samp, k, ni, _ = sample_workload(w, rate * seconds)
-    r = oracle.contract(samp.expr, 1.0, H(samp.A), H(samp.B), 0.0, H(samp.C), nthreads=nthreads, ref=use_ref,
-                        lapack_blocks=not use_ref)
-    desc = (f"A restricted to i-blocks 0..{k - 1} of {ni}: {len(r.pairs)} pairs, {r.flops / 1e9:.2f} GFLOP "
-            f"({'reference Utils::reshape + OpenBLAS dgemm per pair' if use_ref else 'oracle LAPACK-path restatement'}, "
-            f"OpenMP over C blocks)")
-    return r.flops / r.seconds / 1e9, kind, desc, r.seconds
+    samp, k, n0 = sample_workload(w, rate * seconds)
+    vals, secs, flops, npairs = [], [], 0.0, 0
+    for _ in range(max(runs, 1)):
+        r = oracle.contract(samp.expr, 1.0, host(samp.A), host(samp.B), 0.0, host(samp.C), eps=samp.screen_eps,
+                            nthreads=nthreads, ref=ref)
+        vals.append(r.flops / r.seconds / 1e9)
+        secs.append(r.seconds)
+        flops, npairs = r.flops, len(r.pairs)
+    what = ("the reference's Utils::reshape + OpenBLAS dgemm per pair (LAPACK path)" if ref
+            else "the oracle's XMM-order restatement (bit-exact to the asmjit kernel's order)")
+    return {"value": float(np.median(vals)), "unit": "GFLOP/s", "cores": nthreads, "runs": len(vals),
+            "seconds_median": float(np.median(secs)), "kind": "reference" if ref else "port",
+            "sample": (f"A restricted to mode-0 blocks 0..{k - 1} of {n0}: {npairs} pairs, {flops / 1e9:.3f} GFLOP; "
+                       f"{what}; OpenMP over C blocks, {nthreads} thread(s)")}
 
 
 def count_launches(fn):
@@ -200,6 +244,27 @@ def measure_peak(sht, ctx, which):
         return sht.measure_peak(ctx, which)
     except Exception:
         return None
+
+
+def pcie_bandwidth():
+    """Pinned host <-> device copy bandwidth (GB/s) over 1 GiB, best of 3 each way."""
+    import torch
+    n = 1 << 27
+    d = torch.empty(n, dtype=torch.float64, device="cuda")
+    h = torch.empty(n, dtype=torch.float64).pin_memory()
+    out = {}
+    for name, fn in (("h2d", lambda: d.copy_(h, non_blocking=True)), ("d2h", lambda: h.copy_(d, non_blocking=True))):
+        best = 0.0
+        for _ in range(3):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            fn()
+            e1.record()
+            torch.cuda.synchronize()
+            best = max(best, n * 8 / (e0.elapsed_time(e1) * 1e-3) / 1e9)
+        out[name] = best
+    del d, h
+    return out
 
 
 def run_serving(args, sht, ctx, upload, server_kwargs=None):
@@ -313,27 +378,177 @@ def run_serving(args, sht, ctx, upload, server_kwargs=None):
     return out
 
 
+
+# ------------------------------------------------------------------------------ device legs
+FORMS = {"plain": 0, "batched": 1, "split": 2}
+
+
+def form_mode(sht, fname):
+    return {"plain": sht.Mode.PLAIN_FP64, "batched": sht.Mode.BATCHED_FP64, "split": sht.Mode.SPLIT}[fname]
+
+
+def time_contract(sht, ctx, w, A, B, C, mode, steps, warmup, stream, barrier, max_over_ranks):
+    """Full contractions (plan + execute) back to back: device ms per step (max over ranks)."""
+    import torch
+    rep = None
+    for _ in range(warmup):
+        rep = sht.contract(ctx, w.expr, 1.0, A, B, 0.0, C, w.screen_eps, mode=mode, stream=stream)
+    torch.cuda.synchronize()
+    barrier()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(steps):
+        rep = sht.contract(ctx, w.expr, 1.0, A, B, 0.0, C, w.screen_eps, mode=mode, stream=stream)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    barrier()
+    ctx.stream_sync(stream)  # raises if a split launch recorded a failure
+    return max_over_ranks(e0.elapsed_time(e1)) / steps, rep
+
+
+def time_execute(sht, ctx, w, A, B, C, mode, steps, stream):
+    """Execute-only (plan reused): mean device ms per execute, directly and by graph replay."""
+    import torch
+    plan = sht.Plan(ctx, w.expr, A, B, C, w.screen_eps, mode=mode, stream=stream)
+    out = {}
+    for graph in (False, True):
+        for _ in range(3):
+            plan.execute(1.0, 0.0, stream=stream, graph=graph)
+        ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+        for a, b in ev:
+            a.record(stream)
+            plan.execute(1.0, 0.0, stream=stream, graph=graph)
+            b.record(stream)
+        torch.cuda.synchronize()
+        out["exec_graph_ms" if graph else "exec_ms"] = float(np.mean([a.elapsed_time(b) for a, b in ev]))
+    ctx.stream_sync(stream)
+    rep = plan.report()
+    plan.close()
+    return out, rep
+
+
+def oracle_parity(sht, ctx, w, A, B, forms, T, stream, slices_sweep=()):
+    """Every form on the whole workload against the CPU oracle (the XMM-order restatement, all
+    host cores): pattern and pair list compared exactly, values by bit count and by max abs /
+    relative Frobenius error on the device.  slices_sweep: split slice counts whose error is
+    also measured."""
+    import oracle
+    t0 = time.perf_counter()
+    want = oracle.contract(w.expr, 1.0, host(w.A), host(w.B), 0.0, host(w.C), eps=w.screen_eps)
+    oracle_s = time.perf_counter() - t0
+    from shtensor_b200 import workloads as W
+    Cor = T(W.HostBlockSparse(w.C.block_sizes, want.C.ids, want.C.offsets, want.C.data))
+    nnz = int(want.C.data.size)
+    del want.C.data
+    out = {}
+
+    def one(mode):
+        C = T(w.C)
+        plan = sht.Plan(ctx, w.expr, A, B, C, w.screen_eps, mode=mode, stream=stream)
+        plan.execute(1.0, 0.0, stream=stream)
+        ctx.stream_sync(stream)
+        pairs = plan.pairs()
+        plan.close()
+        ids, offs, _ = C.get_sparse_info()
+        res = {"pattern_equal": bool(np.array_equal(ids, want.C.ids) and np.array_equal(offs, want.C.offsets)),
+               "pairs_equal": bool(np.array_equal(pairs, want.pairs))}
+        if res["pattern_equal"]:
+            mx, fro = sht.compare(C, Cor, stream=stream)
+            res.update(max_abs=mx, rel_fro=fro, bits_differ=sht.bitdiff(C, Cor, stream=stream))
+        del C
+        return res
+
+    for f in forms:
+        out[f] = one(form_mode(sht, f))
+    sweep = {}
+    for S in slices_sweep:
+        ctx.set_split_slices(S)
+        try:
+            r = one(sht.Mode.SPLIT)
+            sweep[str(S)] = {"rel_fro": r.get("rel_fro"), "max_abs": r.get("max_abs")}
+        finally:
+            ctx.set_split_slices(7)
+    del Cor
+    return out, sweep, {"seconds": oracle_s, "pairs": int(len(want.pairs)), "c_nnz": nnz,
+                        "kind": "oracle XMM-order restatement, OpenMP over C blocks"}
+
+
+def roofline_of(fname, flops, kern_ms, peaks, S=7):
+    """Achieved rate of the form's kernels against the measured peak of the pipe that bounds it."""
+    tf = flops / kern_ms / 1e9  # TFLOP/s (FP64-equivalent)
+    if fname == "split":
+        ach = flops * S * (S + 1) / 2 / kern_ms / 1e9
+        pk = peaks.get("int8")
+        return {"bound": "tensor", "pipe": f"int8 (tcgen05 kind::i8, {S} slices) with FP64 reassembly",
+                "achieved": ach, "peak": pk, "unit": "TOPS", "frac": ach / pk if pk else None,
+                "fp64_equivalent": {"achieved": tf, "peak": peaks.get("dmma"), "unit": "TFLOP/s",
+                                    "frac": tf / peaks["dmma"] if peaks.get("dmma") else None,
+                                    "peak_source": "FP64 tensor-core (mma.sync m8n8k4) probe, this run"}}
+    if fname == "batched":
+        pk = peaks.get("dmma")
+        return {"bound": "tensor", "pipe": "fp64 tensor core (mma.sync m8n8k4)", "achieved": tf, "peak": pk,
+                "unit": "TFLOP/s", "frac": tf / pk if pk else None}
+    pk = peaks.get("fp64")
+    return {"bound": "tensor", "pipe": "fp64 FMA (DFMA)", "achieved": tf, "peak": pk, "unit": "TFLOP/s",
+            "frac": tf / pk if pk else None}
+
+
+def workload_leg(sht, ctx, w, forms, steps, warmup, stream, T, barrier, max_over_ranks, world, peaks,
+                 check=True, tol=1e-12, sweep=(), autotune=False):
+    """Time every form on one workload (full contraction and execute-only), check each against
+    the oracle and give its roofline."""
+    A, B, C = T(w.A), T(w.B), T(w.C)
+    res = {}
+    flops = None
+    for fname in forms:
+        mode = form_mode(sht, fname)
+        if fname == "batched" and autotune:
+            tuner = sht.Plan(ctx, w.expr, A, B, C, w.screen_eps, mode=mode, stream=stream)
+            tuner.autotune(stream=stream)
+            tuner.close()
+        ms, rep = time_contract(sht, ctx, w, A, B, C, mode, steps, warmup, stream, barrier, max_over_ranks)
+        flops = rep["flops"]
+        ex, prep = time_execute(sht, ctx, w, A, B, C, mode, steps, stream)
+        r = {"ms_per_step": ms, "gflops": world * flops / ms / 1e6, "plan_ms": rep["plan_ms"],
+             "npairs": rep["npairs"], "tiles": rep["nwork"], **ex,
+             "exec_gflops": flops / ex["exec_ms"] / 1e6, "kernel": FORM_KERNEL[fname]}
+        r["roofline"] = roofline_of(fname, prep["flops"], ex["exec_ms"], peaks, prep.get("slices") or 7)
+        res[fname] = r
+    sweep_out, oinfo = {}, None
+    if check:
+        par, sweep_out, oinfo = oracle_parity(sht, ctx, w, A, B, list(res), T, stream, sweep)
+        for f, v in par.items():
+            res[f]["error_vs_oracle"] = v
+            exact = v["pattern_equal"] and v["pairs_equal"]
+            res[f]["fp64_accurate"] = bool(exact and v.get("rel_fro", 1.0) <= tol) if f == "split" else \
+                bool(exact and v.get("bits_differ", 1) == 0)
+    del A, B, C
+    return res, flops, sweep_out, oinfo
+
+
 # ------------------------------------------------------------------------------ arms
 def run_reference(args):
     rank, world, _ = dist_env()
     if rank != 0:
         return
     nthreads = os.cpu_count() or 1
-    w = build_workload(args)
+    w = build_workload(args.workload, args.seed, args.scale)
     vals = []
-    kind = desc = None
+    leg = None
     for _ in range(args.warmup):
-        cpu_reference_run(w, max(args.cpu_sample_seconds / 5, 1.0), nthreads)
+        cpu_leg(w, max(args.cpu_sample_seconds / 5, 1.0), nthreads, True, 1)
     for _ in range(args.steps):
-        v, kind, desc, secs = cpu_reference_run(w, args.cpu_sample_seconds / max(args.steps, 1), nthreads)
-        vals.append(v)
+        leg = cpu_leg(w, args.cpu_sample_seconds / max(args.steps, 1), nthreads, True, 1)
+        vals.append(leg["value"])
     value = float(np.median(vals))
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": "GFLOP/s", "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
-        "config": {"workload": WORKLOAD, "scale": args.scale, "seed": args.seed},
-        "cpu_baseline": {"value": value, "unit": "GFLOP/s", "cores": nthreads, "kind": kind, "sample": desc},
+        "config": {"workload": WORKLOADS[args.workload], "scale": args.scale, "seed": args.seed},
+        "cpu_baseline": {"value": value, "unit": "GFLOP/s", "cores": nthreads, "kind": "reference",
+                         "sample": leg["sample"]},
         "e2e": {"value": value, "unit": "GFLOP/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -352,7 +567,6 @@ def run_ours(args):
     else:
         torch.cuda.set_device(0)
     dev = torch.cuda.current_device()
-    w = build_workload(args)
     ctx = sht.Context(int(args.pool_gb * (1 << 30)), device=dev)
     stream = torch.cuda.current_stream()
 
@@ -363,84 +577,52 @@ def run_ours(args):
             t.upload(h.data)
         return t
 
-    A, B = T(w.A), T(w.B)
-    Cd = T(w.C)
-
     def barrier():
         if world > 1:
             torch.distributed.barrier()
 
-    max_over_ranks = reduce_max
+    forms = [f for f in args.forms.split(",") if f]
+    peaks = {k: measure_peak(sht, ctx, k) for k in ("fp64", "dmma", "int8")}
+    w = build_workload(args.workload, args.seed, args.scale)
+    check = not args.no_oracle and world == 1 and rank == 0
 
-    forms = {"plain": sht.Mode.PLAIN_FP64, "batched": sht.Mode.BATCHED_FP64, "split": sht.Mode.SPLIT}
-    results = {}
-    clocks = None
-    flops = None
-    for fname in [f for f in args.forms.split(",") if f]:
-        mode = forms[fname]
-        rep = None
-        if fname == "batched" and not args.no_autotune:
-            tuner = sht.Plan(ctx, w.expr, A, B, Cd, mode=mode, stream=stream)
-            tuner.autotune(stream=stream)
-            tuner.close()
-        for _ in range(args.warmup):
-            rep = sht.contract(ctx, w.expr, 1.0, A, B, 0.0, Cd, mode=mode, stream=stream)
-        torch.cuda.synchronize()
-        barrier()
-        torch.cuda.synchronize()
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        with ClockSampler(dev) as cs:
-            e0.record(stream)
-            for _ in range(args.steps):
-                rep = sht.contract(ctx, w.expr, 1.0, A, B, 0.0, Cd, mode=mode, stream=stream)
-            e1.record(stream)
-            torch.cuda.synchronize()
-        barrier()
-        ms = max_over_ranks(e0.elapsed_time(e1)) / args.steps
-        flops = rep["flops"]
-        results[fname] = {"ms_per_step": ms, "gflops": world * flops / ms / 1e6, "plan_ms": rep["plan_ms"],
-                          "npairs": rep["npairs"], "tiles": rep["nwork"]}
-        if clocks is None or fname == "batched":
-            clocks = cs.summary()
-    # error of the split form against the FP64 result (both computed on the device)
-    if "split" in results:
-        # reference: the plain FP64 form (the drop-in, bit-exact to the XMM order); the batched
-        # form must equal it bit for bit, and the split form must be within split_tol of it
-        Cref = T(w.C)
-        sht.contract(ctx, w.expr, 1.0, A, B, 0.0, Cref, mode=sht.Mode.PLAIN_FP64, stream=stream)
-        Cb = T(w.C)
-        sht.contract(ctx, w.expr, 1.0, A, B, 0.0, Cb, mode=sht.Mode.BATCHED_FP64, stream=stream)
-        sht.contract(ctx, w.expr, 1.0, A, B, 0.0, Cd, mode=sht.Mode.SPLIT, stream=stream)
-        mx, fro = sht.compare(Cd, Cref, stream=stream)
-        bmx, _ = sht.compare(Cb, Cref, stream=stream)
-        results["split"]["error_vs_fp64"] = {"max_abs": mx, "rel_fro": fro, "slices": 7,
-                                             "reference": "plain FP64 form"}
-        results["split"]["fp64_accurate"] = bool(fro <= args.split_tol)
-        if "batched" in results:
-            results["batched"]["max_abs_vs_plain"] = bmx
-        del Cref, Cb
+    # ---- headline workload: every form timed, checked against the oracle, clocks sampled
+    with ClockSampler(dev) as cs:
+        results, flops, sweep, oinfo = workload_leg(
+            sht, ctx, w, forms, args.steps, args.warmup, stream, T, barrier, reduce_max, world, peaks, check=check,
+            tol=args.split_tol, sweep=(5, 6) if "split" in forms else (), autotune=not args.no_autotune)
+    clocks = cs.summary()
     eligible = [k for k in results if results[k].get("fp64_accurate", True)]
     best = max(eligible, key=lambda k: results[k]["gflops"])
+    if "split" in results:
+        sweep["7"] = {k: results["split"].get("error_vs_oracle", {}).get(k) for k in ("rel_fro", "max_abs")}
+    ratios = {}
+    if "split" in results and "batched" in results:
+        ratios["split_over_batched"] = results["split"]["gflops"] / results["batched"]["gflops"]
+        ratios["split_over_batched_exec"] = results["split"]["exec_gflops"] / results["batched"]["exec_gflops"]
+    if "split" in results and "plain" in results:
+        ratios["split_over_plain"] = results["split"]["gflops"] / results["plain"]["gflops"]
+        ratios["split_over_plain_exec"] = results["split"]["exec_gflops"] / results["plain"]["exec_gflops"]
 
-    # execute-only timing (plan reused) of every form; the best form's kernel gives the roofline
-    exec_ms = {}
-    for fname in results:
-        plan = sht.Plan(ctx, w.expr, A, B, Cd, mode=forms[fname], stream=stream)
-        for _ in range(3):
-            plan.execute(1.0, 0.0, stream=stream)
-        ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
-        for a, b in ev:
-            a.record(stream)
-            plan.execute(1.0, 0.0, stream=stream)
-            b.record(stream)
-        torch.cuda.synchronize()
-        exec_ms[fname] = float(np.mean([a.elapsed_time(b) for a, b in ev]))
-        results[fname]["exec_ms"] = exec_ms[fname]
-        results[fname]["exec_gflops"] = flops / exec_ms[fname] / 1e6
-        prep = plan.report()
-        plan.close()
-        del plan
-    kern_ms = exec_ms[best]
+    # ---- the other configurations
+    configs = {}
+    if not args.no_configs and world == 1:
+        for name in [n for n in ("c0", "c2", "c3") if n != args.workload]:
+            wx = build_workload(name, args.seed, args.scale)
+            fx = {"c0": forms, "c2": [f for f in forms if f in ("batched", "split")],
+                  "c3": [f for f in forms if f in ("batched", "split")]}[name]
+            rx, flx, swx, ox = workload_leg(sht, ctx, wx, fx, max(3, args.steps // 2), args.warmup, stream, T, barrier,
+                                            reduce_max, world, peaks, check=check, tol=args.split_tol,
+                                            sweep=(5, 6) if name in ("c2", "c3") and "split" in fx else ())
+            if "split" in rx:
+                swx["7"] = {k: rx["split"].get("error_vs_oracle", {}).get(k) for k in ("rel_fro", "max_abs")}
+            configs[name] = {"workload": WORKLOADS[name], "gflop_per_step": flx / 1e9, "forms": rx,
+                             "split_slices_error": swx or None, "oracle": ox}
+            del wx
+
+    A, B, Cd = T(w.A), T(w.B), T(w.C)
+    sht.contract(ctx, w.expr, 1.0, A, B, 0.0, Cd, w.screen_eps, mode=form_mode(sht, best), stream=stream)
+    ctx.stream_sync(stream)
     c_nnz = Cd.nnz
     # serving runs before the launch count (the CUPTI profiler it uses slows later launches),
     # the CPU baseline (its OpenMP threads) and the end-to-end copies
@@ -448,40 +630,27 @@ def run_ours(args):
     if world == 1 and not args.no_serving:
         serving = run_serving(args, sht, ctx, T)
     launches, names = (None, []) if args.no_count else count_launches(
-        lambda: sht.contract(ctx, w.expr, 1.0, A, B, 0.0, Cd, mode=forms[best], stream=stream))
-    peak = measure_peak(sht, ctx, "fp64")
-    achieved = prep["flops"] / kern_ms / 1e9  # TFLOP/s
+        lambda: sht.contract(ctx, w.expr, 1.0, A, B, 0.0, Cd, w.screen_eps, mode=form_mode(sht, best), stream=stream))
+    kern = results[best]
+    roofline = dict(kern["roofline"])
     traffic = None
     try:  # DRAM bytes per launch of the dominant kernel, from the committed ncu summary
         with open(os.path.join(ROOT, "profiles", "roofline_traffic.json")) as f:
             traffic = json.load(f).get(best, {}).get("traffic_bytes_per_launch")
     except (OSError, ValueError):
         traffic = None
-    common = {"traffic": traffic,
-              "traffic_source": "profiles/roofline_traffic.json (ncu capture at scale 0.5, scaled to the full workload)",
-              "algorithmic_bytes": 8.0 * (c_nnz + w.A.nnz + w.B.nnz), "kernel_ms": kern_ms,
-              "kernel": {"plain": "k_contract_tiles", "batched": "k_matform + k_batched",
-                         "split": "k_slice + k_split"}.get(best, best)}
-    fp64_line = {"achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": (achieved / peak) if peak else None,
-                 "peak_source": "measured in this run by the library's FP64 FMA-chain kernel" if peak else "unmeasured"}
-    if best == "split":
-        # the split kernel's bound is the INT8 tensor core: S(S+1)/2 slice products per FP64 flop
-        S = int(results["split"].get("error_vs_fp64", {}).get("slices", 7))
-        int8_peak = measure_peak(sht, ctx, "int8")
-        int8_ach = prep["flops"] * S * (S + 1) / 2 / kern_ms / 1e9  # TOPS
-        roofline = {"bound": "tensor", "pipe": f"int8 (tcgen05 kind::i8, {S} slices) with FP64 reassembly",
-                    "achieved": int8_ach, "peak": int8_peak, "unit": "TOPS",
-                    "frac": (int8_ach / int8_peak) if int8_peak else None,
-                    "peak_source": "measured in this run by the library's tcgen05 kind::i8 kernel" if int8_peak
-                    else "unmeasured",
-                    "fp64_equivalent": fp64_line, **common}
-    else:
-        roofline = {"bound": "tensor", "pipe": "fp64 (DFMA / DMMA; B200's FP64 and FP64-tensor peaks are the same figure)",
-                    **fp64_line, **common}
+    roofline.update({"traffic": traffic,
+                     "traffic_source": "profiles/roofline_traffic.json (ncu capture of a smaller case of the same "
+                                       "kernel, scaled to the full workload)",
+                     "algorithmic_bytes": 8.0 * (c_nnz + w.A.nnz + w.B.nnz), "kernel_ms": kern["exec_ms"],
+                     "kernel": FORM_KERNEL[best],
+                     "peak_source": "measured in this run by the library's own probe kernels "
+                                    "(tcgen05 kind::i8 / mma.sync m8n8k4 / DFMA chains)"})
 
     # end to end through the public API: host buffers in pinned memory, copies timed
     e2e = None
     if not args.no_e2e:
+        bw = pcie_bandwidth()
         ha = torch.from_numpy(w.A.data).pin_memory()
         hb = torch.from_numpy(w.B.data).pin_memory()
         hc = torch.empty(Cd.nnz, dtype=torch.float64).pin_memory()
@@ -494,20 +663,27 @@ def run_ours(args):
         for _ in range(nrep):
             A.upload(ha.numpy(), stream=stream)
             B.upload(hb.numpy(), stream=stream)
-            sht.contract(ctx, w.expr, 1.0, A, B, 0.0, Cd, mode=forms[best], stream=stream)
+            sht.contract(ctx, w.expr, 1.0, A, B, 0.0, Cd, w.screen_eps, mode=form_mode(sht, best), stream=stream)
             Cd.download(hc.numpy(), stream=stream)
         ee1.record(stream)
         torch.cuda.synchronize()
-        ms = max_over_ranks(ee0.elapsed_time(ee1)) / nrep
-        e2e = {"value": world * flops / ms / 1e6, "unit": "GFLOP/s",
-               "h2d_bytes_per_step": int(ha.numel() * 8 + hb.numel() * 8), "d2h_bytes_per_step": int(hc.numel() * 8),
-               "ms_per_step": ms, "wall_ms_per_step": (time.perf_counter() - t0) * 1e3 / nrep}
+        ms = reduce_max(ee0.elapsed_time(ee1)) / nrep
+        h2d, d2h = int(ha.numel() * 8 + hb.numel() * 8), int(hc.numel() * 8)
+        floor_ms = (h2d / bw["h2d"] + d2h / bw["d2h"]) / 1e6
+        e2e = {"value": world * flops / ms / 1e6, "unit": "GFLOP/s", "h2d_bytes_per_step": h2d,
+               "d2h_bytes_per_step": d2h, "ms_per_step": ms, "wall_ms_per_step": (time.perf_counter() - t0) * 1e3 / nrep,
+               "copy_floor_ms": floor_ms, "pcie_gbs": bw,
+               "note": "the copies alone (pinned, measured bandwidth) take copy_floor_ms per step"}
+        del ha, hb, hc
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
-        v, kind, desc, secs = cpu_reference_run(w, args.cpu_sample_seconds, os.cpu_count() or 1)
-        cpu = {"value": v, "unit": "GFLOP/s", "cores": os.cpu_count(), "kind": kind, "sample": desc,
-               "seconds": secs}
+        ncores = os.cpu_count() or 1
+        legs = {"reference_openmp": cpu_leg(w, args.cpu_sample_seconds / args.cpu_runs, ncores, True, args.cpu_runs),
+                "reference_1thread": cpu_leg(w, 2.0, 1, True, args.cpu_runs),
+                "xmm_restatement_1thread": cpu_leg(w, 2.0, 1, False, args.cpu_runs)}
+        cpu = dict(legs["reference_openmp"])
+        cpu["legs"] = legs
 
     del A, B, Cd
 
@@ -517,14 +693,14 @@ def run_ours(args):
             "metric": METRIC, "value": r["gflops"], "unit": "GFLOP/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": r["ms_per_step"], "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
-            "config": {"workload": WORKLOAD, "form": best, "scale": args.scale, "seed": args.seed,
-                       "npairs": r["npairs"], "gflop_per_step": flops / 1e9,
-                       "l2": "inputs and output larger than L2 (A+B 168 MB, C 5.9 GB); no flush",
-                       "c_nnz": c_nnz,
-                       "parallelism": f"replicas x{world}"},
-            "forms": results, "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "clocks": clocks,
+            "config": {"workload": WORKLOADS[args.workload], "name": args.workload, "form": best, "scale": args.scale,
+                       "seed": args.seed, "npairs": r["npairs"], "gflop_per_step": flops / 1e9,
+                       "l2": "inputs and output larger than L2 (C alone is GBs); no flush",
+                       "c_nnz": c_nnz, "parallelism": f"replicas x{world}"},
+            "forms": results, "ratios": ratios, "split_slices_error": sweep or None, "oracle": oinfo,
+            "roofline": roofline, "peaks": peaks, "cpu_baseline": cpu, "e2e": e2e, "clocks": clocks,
             "gpu_launches": (launches * args.steps) if launches is not None else None,
-            "gpu_launches_per_step": launches, "serving": serving,
+            "gpu_launches_per_step": launches, "configs": configs or None, "serving": serving,
         }
         print(json.dumps(line), flush=True)
     ctx.close()

@@ -176,6 +176,20 @@ sht_status sht_autotune(sht_plan* p, const char* cache_file, void* stream);
 /* INT8 slices per operand used by SHT_MODE_SPLIT plans made after the call (1..8, default 7) */
 sht_status sht_set_split_slices(sht_ctx* ctx, int slices);
 
+/* Split mode is asynchronous like the FP64 forms: sht_contract and sht_plan_execute return once
+ * the work is queued on `stream`.  The split kernel's pipeline waits are bounded; a wait that
+ * runs out (a hardware or scheduling fault) leaves C undefined and records SHT_ERR_TIMEOUT on
+ * the context.  The next split call on the context reports it (without queueing its own work),
+ * and sht_stream_sync reports it after the stream's work is done.  Non-finite inputs are not an
+ * error: such an execute is computed by the FP64 tiles, with IEEE propagation as in the FP64
+ * forms. */
+/* waits for the work queued on `stream`, then returns (and clears) the first failure recorded
+ * by this context's device work, if any */
+sht_status sht_stream_sync(sht_ctx* ctx, void* stream);
+/* diagnostic: polls of one device pipeline wait of the split kernel before the launch gives up
+ * (0 = the default, about a second); waits for work already issued keep their own bound */
+sht_status sht_set_wait_limit(sht_ctx* ctx, int64_t polls);
+
 /* ---- diagnostics ---- */
 /* which = 0: FP64 FMA peak of this GPU in TFLOP/s (the FP64 kernels' roofline denominator);
  * which = 1: dense INT8 tensor-core (tcgen05 kind::i8) peak in TOPS (the split kernel's);

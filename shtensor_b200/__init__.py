@@ -136,6 +136,8 @@ _SIGS = {
     "sht_autotune": [_P, C.c_char_p, _P],
     "sht_measure_peak": [_P, C.c_int, C.POINTER(C.c_double)],
     "sht_set_split_slices": [_P, C.c_int],
+    "sht_stream_sync": [_P, _P],
+    "sht_set_wait_limit": [_P, C.c_int64],
     "sht_server_create": [_P, C.POINTER(ServerConfig), C.POINTER(_P)],
     "sht_server_submit": [_P, C.c_char_p, C.c_double, _P, _P, C.c_double, _P, C.c_double, C.c_int,
                           C.POINTER(C.c_int64)],
@@ -223,6 +225,16 @@ class Context:
     def set_split_slices(self, slices: int):
         """INT8 slices per operand of split-precision plans made afterwards (1..8)."""
         _check(lib().sht_set_split_slices(self._h, slices))
+
+    def stream_sync(self, stream=None):
+        """Wait for the work queued on `stream` and raise the first failure this context's
+        device work recorded (a split launch whose bounded wait ran out)."""
+        _check(lib().sht_stream_sync(self._h, _stream(stream)))
+
+    def set_wait_limit(self, polls: int):
+        """Diagnostic: polls of one split-kernel pipeline wait before the launch gives up (0 =
+        default)."""
+        _check(lib().sht_set_wait_limit(self._h, int(polls)))
 
     def configure_pool(self, chunk_header: int, alignment: int):
         _check(lib().sht_pool_configure(self._h, chunk_header, alignment))

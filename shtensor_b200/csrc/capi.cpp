@@ -55,12 +55,18 @@ static void contract_split(sht_plan* p, double alpha, double beta, cudaStream_t 
   split_layout(p, ctx->split_slices ? ctx->split_slices : split_slices_default(), s);
   split_slice(p, alpha, s);
   trace("contract: slicer launched", s);
-  SHT_CUDA(cudaStreamWaitEvent(ps, lane.lane.start, 0));
+  // The build reads the tensors' indices (complete: every index change in this library returns
+  // after it is done) and, with screening, A's and B's values, which earlier work on s may still
+  // write: only then does it wait for s.  So a contraction into a C whose pattern holds the
+  // product plans while the previous contraction on s still runs.
+  if (p->eps > 0.0) SHT_CUDA(cudaStreamWaitEvent(ps, lane.lane.start, 0));
   try {
     plan_build(p, ps, true);
     split_records(p, ps);
   } catch (const PatternGrew&) {
-    // the product adds blocks to C: build again, growing C's pattern
+    // the product adds blocks to C: build again, growing C's pattern, which moves C's values
+    // (after earlier work on s has written them)
+    SHT_CUDA(cudaStreamWaitEvent(ps, lane.lane.start, 0));
     plan_build(p, ps, false);
     split_records(p, ps);
   }
@@ -69,8 +75,13 @@ static void contract_split(sht_plan* p, double alpha, double beta, cudaStream_t 
   plan_touch(p, s);
   split_launch(p, sparse_args(p, alpha, beta), s);
   trace("contract: split kernel launched", s);
-  split_check(p, s);
-  trace("contract: checked", s);
+}
+
+// A bounded wait of an earlier split launch on this context ran out: report it at this call.
+static void raise_pending(sht_ctx* ctx) {
+  if (const int e = ctx_take_error(ctx))
+    fail((sht_status)e, "an earlier split-precision launch on this context failed: a bounded wait on the tensor "
+                        "cores expired (its result is undefined)");
 }
 
 // Batched form of sht_contract, overlapped the same way: the matrix form of A and B (patterns
@@ -87,11 +98,13 @@ static void contract_batched(sht_plan* p, double alpha, double beta, cudaStream_
   std::memcpy(&ab, &alpha, 8);
   if (ab != 0) matform_execute(p, alpha, s);
   trace("contract: matrix form launched", s);
-  SHT_CUDA(cudaStreamWaitEvent(ps, lane.lane.start, 0));
+  // as in the split form: the build waits for earlier work on s only when it reads values
+  if (p->eps > 0.0) SHT_CUDA(cudaStreamWaitEvent(ps, lane.lane.start, 0));
   try {
     plan_build(p, ps, true);
     device_work_list(p, 0, 0, true, ps);
   } catch (const PatternGrew&) {
+    SHT_CUDA(cudaStreamWaitEvent(ps, lane.lane.start, 0));
     plan_build(p, ps, false);
     device_work_list(p, 0, 0, true, ps);
   }
@@ -105,6 +118,29 @@ static void contract_batched(sht_plan* p, double alpha, double beta, cudaStream_
 static void prepare_mode(sht_plan* p, cudaStream_t s) {
   if (p->mode == SHT_MODE_BATCHED_FP64) batched_prepare(p, s);
   if (p->mode == SHT_MODE_SPLIT) split_prepare(p, p->ctx->split_slices ? p->ctx->split_slices : split_slices_default(), s);
+}
+
+volatile int* ctx_error_word(sht_ctx* ctx) {
+  std::lock_guard<std::mutex> lk(ctx->err_mu);
+  if (!ctx->err_host) {
+    void* h = nullptr;
+    SHT_CUDA(cudaHostAlloc(&h, 64, cudaHostAllocMapped));
+    std::memset(h, 0, 64);
+    void* d = nullptr;
+    SHT_CUDA(cudaHostGetDevicePointer(&d, h, 0));
+    ctx->err_host = static_cast<int*>(h);
+    ctx->err_dev = static_cast<int*>(d);
+  }
+  return ctx->err_dev;
+}
+
+int ctx_take_error(sht_ctx* ctx) {
+  std::lock_guard<std::mutex> lk(ctx->err_mu);
+  if (!ctx->err_host) return 0;
+  volatile int* w = ctx->err_host;
+  const int e = *w;
+  if (e) *w = 0;
+  return e;
 }
 
 static thread_local std::string g_last_error;
@@ -143,6 +179,7 @@ sht_status sht_init(sht_ctx** out, int device, size_t pool_bytes) {
     c->num_sms = sms;
     c->pool = std::make_shared<DevicePool>(device, pool_bytes);
     SHT_CUDA(cudaStreamCreateWithFlags(&c->stage_stream, cudaStreamNonBlocking));
+    ctx_error_word(c.get());  // the device error word exists before any capture
     *out = c.release();
   });
 }
@@ -152,6 +189,7 @@ sht_status sht_finalize(sht_ctx* ctx) {
     if (!ctx) return;
     cudaDeviceSynchronize();
     if (ctx->stage_stream) cudaStreamDestroy(ctx->stage_stream);
+    if (ctx->err_host) cudaFreeHost(ctx->err_host);
     for (auto& l : ctx->lanes) {
       cudaEventDestroy(l.start);
       cudaEventDestroy(l.done);
@@ -451,9 +489,8 @@ sht_status sht_plan_create(sht_ctx* ctx, const char* expr, sht_tensor* A, sht_te
 sht_status sht_plan_execute(sht_plan* p, double alpha, double beta, void* stream) {
   return guard([&] {
     need(p, "null plan");
+    if (p->mode == SHT_MODE_SPLIT) raise_pending(p->ctx);
     plan_execute(p, alpha, beta, as_stream(stream));
-    // split mode reports its bounded-wait and input checks synchronously
-    if (p->mode == SHT_MODE_SPLIT) split_check(p, as_stream(stream));
   });
 }
 
@@ -495,8 +532,7 @@ sht_status sht_plan_report(sht_plan* p, sht_contract_report* rep) {
     rep->nblocks_c = p->C->nblocks;
     rep->nnz_c = p->C->nnz;
     rep->nwork = p->mode == SHT_MODE_BATCHED_FP64 ? p->bwork : p->nwork;
-    if (p->flops_pending) SHT_CUDA(cudaDeviceSynchronize());  // the plan's stream is not known here
-    rep->flops = plan_flops(p, p->ctx->stage_stream);
+    rep->flops = plan_flops(p, p->ctx->stage_stream);  // waits for the count's own event
     rep->plan_ms = p->plan_ms;
     rep->exec_ms = p->exec_ms;
     rep->slices = p->split_slices;
@@ -538,6 +574,7 @@ sht_status sht_contract(sht_ctx* ctx, const char* expr, double alpha, sht_tensor
     need(norm >= SHT_NORM_FROBENIUS && norm <= SHT_NORM_FROBENIUS_REFCOMPAT, "unknown norm");
     cudaStream_t s = as_stream(stream);
     std::unique_ptr<sht_plan> p;
+    if (mode == SHT_MODE_SPLIT) raise_pending(ctx);
     if (mode == SHT_MODE_SPLIT) {
       p.reset(plan_init(ctx, expr, A, B, C, eps, norm, mode, s));
       contract_split(p.get(), alpha, beta, s);
@@ -592,6 +629,24 @@ sht_status sht_set_split_slices(sht_ctx* ctx, int slices) {
     need(ctx, "null context");
     if (slices < 1 || slices > 8) fail(SHT_ERR_INVALID, "split slices must be 1..8");
     ctx->split_slices = slices;
+  });
+}
+
+sht_status sht_set_wait_limit(sht_ctx* ctx, int64_t polls) {
+  return guard([&] {
+    need(ctx, "null context");
+    need(polls >= 0, "wait limit must be >= 0");
+    ctx->wait_limit = polls;
+  });
+}
+
+sht_status sht_stream_sync(sht_ctx* ctx, void* stream) {
+  return guard([&] {
+    need(ctx, "null context");
+    SHT_CUDA(cudaStreamSynchronize(as_stream(stream)));
+    if (const int e = ctx_take_error(ctx))
+      fail((sht_status)e, "a split-precision launch on this context failed: a bounded wait on the tensor cores "
+                          "expired (its result is undefined)");
   });
 }
 

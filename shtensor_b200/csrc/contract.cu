@@ -240,6 +240,40 @@ static void launch_tiles(int cfg, long long nwork, const SparseArgs& g, cudaStre
   SHT_CUDA(cudaGetLastError());
 }
 
+// The FP64 tiles of a split plan's work list, computed only when the device word *flag is set
+// (an operand of the execute holds a non-finite value): persistent, one 128 x 32 tile per
+// iteration, the same tiles and element order as the plain form.
+__global__ void __launch_bounds__(Cfg128x32::kThreads) k_contract_tiles_if(SparseArgs g, const int4* __restrict__ work,
+                                                                            int nwork, const int* __restrict__ flag) {
+  if (*flag == 0) return;
+  __shared__ TileSmem<double, Cfg128x32> sm;
+  for (int i = blockIdx.x; i < nwork; i += gridDim.x) {
+    const int4 w = work[i];
+    const int c = w.x;
+    auto getc = [&](double*& p, const int*& d) {
+      p = g.C + g.offC[c];
+      d = g.dimsC + (long long)c * g.mp.oC;
+    };
+    auto getpair = [&](int p, const double*& a, const int*& ad, const double*& b, const int*& bd) {
+      const int ia = g.pair_a[p], ib = g.pair_b[p];
+      a = g.A + g.offA[ia];
+      ad = g.dimsA + (long long)ia * g.mp.oA;
+      b = g.B + g.offB[ib];
+      bd = g.dimsB + (long long)ib * g.mp.oB;
+    };
+    tile_run<double, Cfg128x32>(g.mp, g.sc, w.y, getc, getpair, g.pstart[c], g.pstart[c + 1], sm);
+    __syncthreads();  // the next tile reuses the shared tables
+  }
+}
+
+void fallback_tiles_if(const SparseArgs& g, const int4* work, long long nwork, const int* flag, int grid,
+                       cudaStream_t s) {
+  if (nwork <= 0) return;
+  k_contract_tiles_if<<<(unsigned)std::min<long long>(grid, nwork), Cfg128x32::kThreads, 0, s>>>(g, work, (int)nwork,
+                                                                                               flag);
+  SHT_CUDA(cudaGetLastError());
+}
+
 // Count the product block ids (sorted, with repeats) that are absent from the stored C ids
 // (sorted, unique): zero means the result pattern is C's pattern.
 __global__ void k_count_missing(const long long* __restrict__ pc, long long np, const long long* __restrict__ cids,
@@ -364,10 +398,14 @@ void cblock_stats(sht_plan* p, cudaStream_t s) {
   PoolBuf tmp(pool, tb, s);
   cub::DeviceReduce::Sum(tmp.ptr, tb, fl.as<double>(), p->d_flops.as<double>(), (int)nc, s);
   p->flops_pending = true;  // read with the next synchronization (plan_flops)
+  if (!p->flops_event) SHT_CUDA(cudaEventCreateWithFlags(&p->flops_event, cudaEventDisableTiming));
+  SHT_CUDA(cudaEventRecord(p->flops_event, s));
 }
 
 double plan_flops(sht_plan* p, cudaStream_t s) {
   if (p->flops_pending) {
+    // s need not be the stream that computed the count: order the read after it
+    if (p->flops_event) SHT_CUDA(cudaStreamWaitEvent(s, p->flops_event, 0));
     p->flops = d2h_scalar<double>(p->d_flops.ptr, s);
     p->flops_pending = false;
   }
@@ -722,7 +760,7 @@ void plan_touch(sht_plan* p, cudaStream_t s) {
                      &p->mf_b, &p->mf_aoff, &p->mf_boff, &p->mf_ald, &p->mf_bld, &p->mf_ak4, &p->mf_aitems,
                      &p->mf_bitems})
     b->use_on(s);
-  for (PoolBuf* b : {&p->sp_a, &p->sp_b, &p->sp_ae, &p->sp_be, &p->sp_meta, &p->sp_items, &p->sp_pairs,
+  for (PoolBuf* b : {&p->sp_a, &p->sp_b, &p->sp_ae, &p->sp_be, &p->sp_bsc, &p->sp_meta, &p->sp_items, &p->sp_pairs,
                      &p->sp_rowtab, &p->sp_coltab})
     b->use_on(s);
 }

@@ -19,6 +19,7 @@ struct sht_plan {
   sht::PoolBuf d_npairs;            // device pair count, when the host's sized the pair list
   sht::PoolBuf d_missing;           // product blocks absent from C, when the build assumed none
   bool flops_pending = false;       // d_flops not yet copied into flops
+  cudaEvent_t flops_event = nullptr;  // recorded after d_flops is computed
   int shape = 0, work_tm = 64, work_tn = 64;
   sht::PoolBuf d_pair_a, d_pair_b;  // int32 storage indices into A / B, canonical order
   sht::PoolBuf d_pstart;            // int32[ncblk + 1]
@@ -40,12 +41,13 @@ struct sht_plan {
   long long mf_elems = 0;
   // split path: INT8 slices (K-major rows), row / column exponents, error words
   sht::PoolBuf sp_a, sp_b, sp_ae, sp_be;
+  sht::PoolBuf sp_bsc;                // B column scales 2^f as doubles (the reassembly's)
   // one upload: per block of A and of B its slice offset, exponent offset and first slicer
   // item (items of 32 rows), and the kernels' error words (zero)
   sht::PoolBuf sp_meta;
   long long *sp_aoff = nullptr, *sp_aeoff = nullptr, *sp_aistart = nullptr;
   long long *sp_boff = nullptr, *sp_beoff = nullptr, *sp_bistart = nullptr;
-  int* sp_err = nullptr;
+  int* sp_err = nullptr;            // the execute's flag words (non-finite input, wide exponents)
   long long sp_naitems = 0, sp_nbitems = 0;
   sht::PoolBuf sp_items, sp_pairs;    // per-tile and per-pair records of the split kernel
   sht::PoolBuf sp_rowtab, sp_coltab;  // element offsets of every C row / column in its block
@@ -57,6 +59,7 @@ struct sht_plan {
   ~sht_plan() {
     if (graph_exec) cudaGraphExecDestroy(graph_exec);
     if (graph) cudaGraphDestroy(graph);
+    if (flops_event) cudaEventDestroy(flops_event);
   }
 };
 
@@ -111,7 +114,10 @@ void split_records(sht_plan* p, cudaStream_t s);
 void split_slice(sht_plan* p, double alpha, cudaStream_t s);
 // the tensor-core kernel: needs everything above
 void split_launch(sht_plan* p, const SparseArgs& sa, cudaStream_t s);
-void split_check(sht_plan* p, cudaStream_t s);
+// The FP64 tile kernel over the split work list (int4 (C block, 128 x 32 tile, ., .)), run only
+// when the device word *flag is set (persistent grid; it returns at once otherwise).
+void fallback_tiles_if(const SparseArgs& g, const int4* work, long long nwork, const int* flag, int grid,
+                       cudaStream_t s);
 int split_slices_default();
 void matform_execute(sht_plan* p, double alpha, cudaStream_t s);
 void block_dims_sizes(const sht_tensor* t, const long long* ids, long long n, int* dims, long long* sizes,

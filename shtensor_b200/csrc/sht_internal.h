@@ -173,6 +173,13 @@ struct sht_ctx {
   std::vector<Lane> lanes;
   std::map<std::string, int> tuned;     // autotuner choices: size-class key -> tile id
   int split_slices = 0;                 // INT8 slices per operand in split mode (0 = default)
+  long long wait_limit = 0;             // polls of a device pipeline wait (0 = default)
+  // Error word of device work (a bounded wait of the split kernel that ran out): host memory
+  // mapped into the device, written by a kernel only on failure and read by the host without
+  // a synchronization; sticky until reported (created on first use)
+  int* err_host = nullptr;
+  int* err_dev = nullptr;
+  std::mutex err_mu;
 };
 
 // Parsed einsum: matrix dimension <-> tensor modes (local positions)
@@ -245,6 +252,11 @@ void tensor_compare_device(sht_tensor* X, sht_tensor* R, double* max_abs, double
 // stack kernel (stack.cu)
 void stack_call(sht_kernel* k, const void* a, const void* b, void* c, int64_t nb_ops,
                 cudaStream_t s);
+
+// the context's device error word (host-mapped; created on first use)
+volatile int* ctx_error_word(sht_ctx* ctx);
+// the first device-side failure recorded since the last call (0 if none); clears it
+int ctx_take_error(sht_ctx* ctx);
 
 // timing helpers
 double now_ms();

@@ -39,6 +39,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstddef>
 #include <cstring>
 
 #include "contract.h"
@@ -65,18 +66,29 @@ __host__ __device__ __forceinline__ int slab_offset(int r, int k) {
   return (r >> 3) * 256 + (k >> 4) * 128 + (r & 7) * 16 + (k & 15);
 }
 
+// Flag words of one split execute (device, zeroed before the slicer runs):
+//   [0] set by the slicer when an operand holds a non-finite value: the tensor-core kernel
+//       then writes nothing and the FP64 tile kernel computes the contraction instead;
+//   [1] set when a row or column exponent lies outside the range of the scale-folded
+//       reassembly (A rows: 2^e with -900 <= e <= 960; B columns: 2^e a normal double): the
+//       kernel then scales every element on its own.
+constexpr int kFlagNonFinite = 0, kFlagGeneralExp = 1;
+constexpr int kExpLoA = -900, kExpHiA = 960, kExpLoB = -1022, kExpHiB = 1023;
+
 // One warp per item of 32 rows of one block (lane = row; items are numbered block after block,
 // istart[b] the first item of block b): the row maximum gives the row's
 // exponent (rows padded up to the tile height R get 0), then the S int8 slices of the row
 // go out in tile order: out[((tile * ksteps + ks) * S + t) * R * 32 + slab_offset(row % R, k)].
-// Rows past the block and k past K are zero.
+// Rows past the block and k past K are zero.  With pscale set (B columns), the row's scale 2^e
+// is also written as a double (0 when e is outside [elo, ehi]).
 __global__ void __launch_bounds__(256) k_slice(const double* __restrict__ src, const long long* __restrict__ src_off,
                                                const int* __restrict__ dims, int order, ModeMap fm, ModeMap km,
                                                const long long* __restrict__ out_off,
                                                const long long* __restrict__ exp_off, signed char* __restrict__ out,
-                                               short* __restrict__ expo, double scale, int S, int R,
+                                               short* __restrict__ expo, double* __restrict__ pscale, int elo, int ehi,
+                                               double scale, int S, int R,
                                                const long long* __restrict__ istart, long long nblocks,
-                                               long long nitems, int* __restrict__ bad) {
+                                               long long nitems, int* __restrict__ flags) {
   const int lane = threadIdx.x & 31;
   const long long nwarps = (long long)gridDim.x * (blockDim.x >> 5);
   for (long long it = blockIdx.x * (long long)(blockDim.x >> 5) + (threadIdx.x >> 5); it < nitems; it += nwarps) {
@@ -117,13 +129,16 @@ __global__ void __launch_bounds__(256) k_slice(const double* __restrict__ src, c
     if (live) {
       for (int k = 0; k < K; ++k) {
         const double v = __dmul_rn(s[fr + koff(k)], scale);
-        if (!isfinite(v)) atomicExch(bad, 1);
+        if (!isfinite(v)) atomicExch(&flags[kFlagNonFinite], 1);
         mx = fmax(mx, fabs(v));
       }
     }
     int e = 0;
     if (mx > 0.0) frexp(mx, &e);
     expo[exp_off[b] + r] = (short)e;
+    const bool in_range = e >= elo && e <= ehi;
+    if (!in_range) atomicExch(&flags[kFlagGeneralExp], 1);
+    if (pscale) pscale[exp_off[b] + r] = in_range ? ldexp(1.0, e) : 0.0;
     // pass 2: 16 k at a time; the S slices are packed four bytes to a register and stored
     // as one 16-byte word each
     signed char* o = out + out_off[b] + (long long)(r / R) * ksteps * S * R * kSplitK;
@@ -355,18 +370,22 @@ struct SplitArgs {
   int beta_zero, alpha_zero, S;
   const signed char* As; const short* Ae;  // A slices and row exponents
   const signed char* Bs; const short* Be;  // B slices and column exponents
+  const double* Bsc;                       // B column scales 2^f (0 outside the normal range)
   double* C;
   const int* rowtab; const int* coltab;  // element offsets of C rows / columns
   const SplitItem* items;  // per work item (tile)
   const SplitPair* prs;    // per block pair
   int nwork;
-  int* err;
-  long long wait_limit;
+  const int* flags;        // the execute's flag words (kFlag*)
+  volatile int* err;       // the context's error word (host-mapped): SHT_ERR_TIMEOUT
+  long long wait_limit;    // polls of one pipeline wait before the launch gives up
+  long long drain_limit;   // polls of the waits for work already issued (copies, MMAs)
 };
 
 // Per tile, the producer also copies the tile's record and its row / column offsets into a
-// ring of tile slots, and per pair the A row and B column exponents into a ring of exponent
-// slots, so the epilogue reads nothing from global memory but the C values it scales by beta.
+// ring of tile slots, and per pair the A row exponents, the B column exponents and the B
+// column scales into a ring of exponent slots, so the epilogue reads nothing from global
+// memory but the C values it scales by beta.
 struct SplitTileSlot {
   SplitItem rec;
   int rowoff[kSplitM];
@@ -375,11 +394,12 @@ struct SplitTileSlot {
 struct SplitExpSlot {
   short ea[kSplitM];
   short eb[kSplitN];
+  double sc[kSplitN];
 };
 constexpr unsigned kTileSlotBytes = sizeof(SplitTileSlot);
 constexpr unsigned kExpSlotBytes = sizeof(SplitExpSlot);
 static_assert(sizeof(SplitItem) % 16 == 0 && kTileSlotBytes == 48 + 4 * (kSplitM + kSplitN) &&
-                  kExpSlotBytes == 2 * (kSplitM + kSplitN),
+                  kExpSlotBytes == 2 * (kSplitM + kSplitN) + 8 * kSplitN && offsetof(SplitExpSlot, sc) % 16 == 0,
               "slot members are bulk-copy destinations at 16-byte offsets");
 
 struct SplitSmem {
@@ -399,20 +419,68 @@ __device__ __forceinline__ bool split_wait(void* mbar, unsigned parity, volatile
     if (*abort) return false;
   }
   *abort = 1;
-  atomicExch(g.err, (int)SHT_ERR_TIMEOUT);
+  *g.err = (int)SHT_ERR_TIMEOUT;  // every writer stores the same value
+  __threadfence_system();
   return false;
+}
+
+// bounded wait for work this CTA issued already (bulk copies, MMAs): it always completes, so
+// the bound is generous and no abort flag applies
+__device__ __forceinline__ void split_settle(void* mbar, unsigned parity, const SplitArgs& g) {
+  for (long long i = 0; i < g.drain_limit; ++i)
+    if (mbar_try(mbar, parity)) return;
+}
+
+// Reassembly weights.  Groups are numbered gi = 0..S-1 (group g = gi + 2 of the triangle); the
+// value of one element of one pair is 2^(e_r + f_c) * sum_gi 2^(-7(gi + 2)) P_gi.
+// Narrow launches (every |P_gi| < 2^23) combine the groups two by two in 32 bits,
+// X_k = P_2k * 128 + P_2k+1, with weight 2^(-14k - 21); for odd S >= 3 the last group is
+// folded into the last pair rounded to its weight, X += (P_S-1 + 64) >> 7, an error of at most
+// 2^(-7S - 1) of the row / column scales, below the slicing's own truncation (2^(-7S) per term
+// of the contracted sum); S = 1 keeps X_0 = P_0 with weight 2^-14.
+__host__ __device__ constexpr int narrow_nx(int S) { return S == 1 ? 1 : S / 2; }
+__host__ __device__ constexpr int narrow_wexp(int S, int k) { return S == 1 ? -14 : -14 * k - 21; }
+
+// Loads groups [g0, g1) of this thread's 8 columns from TMEM and folds them into the narrow
+// sums X (groups 2k and 2k+1 into X_k; the odd last group rounded into X_(nx-1)).
+template <int S, int g0, int g1>
+__device__ __forceinline__ void narrow_load(unsigned tb, int (&X)[narrow_nx(S)][8]) {
+  unsigned v[g1 - g0][8];
+#pragma unroll
+  for (int i = 0; i < g1 - g0; ++i) tmem_ld8(tb + (unsigned)((g0 + i) * kSplitN), v[i]);
+  tmem_wait_ld();
+#pragma unroll
+  for (int gi = g0; gi < g1; ++gi) {
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+      const int p = (int)v[gi - g0][j];
+      if (S == 1) {
+        X[0][j] = p;
+      } else if ((S & 1) && gi == S - 1) {
+        X[narrow_nx(S) - 1][j] += (p + 64) >> 7;  // the odd last group, rounded
+      } else if ((gi & 1) == 0) {
+        X[gi >> 1][j] = p * 128;
+      } else {
+        X[gi >> 1][j] += p;
+      }
+    }
+  }
 }
 
 // S (slices per operand) is a template parameter so that the group loops of the MMA issuer
 // and of the reassembly unroll completely; one instance per S = 1..8.  Narrow: every group sum
-// is below 2^23 in magnitude (the host checks S * 127^2 * K), so two groups combine exactly in
-// 32 bits and convert with one integer operation and one FP64 add.
+// is below 2^23 in magnitude (the host checks S * 127^2 * K), so groups combine two by two in
+// 32 bits and each pair converts with one integer operation and one FP64 add.
 template <int S, bool Narrow>
-__global__ void __launch_bounds__(kSplitThreads, 1) k_split(SplitArgs g) {
+__global__ void __maxnreg__(112) k_split(SplitArgs g) {
+  // an operand holds a non-finite value: the FP64 tile kernel computes this execute
+  if (g.flags[kFlagNonFinite]) return;
   extern __shared__ __align__(1024) unsigned char smem_raw[];
   SplitSmem& sm = *reinterpret_cast<SplitSmem*>(smem_raw);
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   volatile int* abort = &sm.abort;
+  // some row or column exponent lies outside the scale-folded range (uniform over the launch)
+  const bool general = g.flags[kFlagGeneralExp] != 0;
 
   if (warp == 0) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&sm.tmem_base)),
@@ -468,6 +536,7 @@ __global__ void __launch_bounds__(kSplitThreads, 1) k_split(SplitArgs g) {
           mbar_expect_tx(&sm.efull[es], kExpSlotBytes);
           bulk_g2s(sm.ex[es].ea, g.Ae + pr.ae_off + t.r0, 2 * kSplitM, &sm.efull[es]);
           bulk_g2s(sm.ex[es].eb, g.Be + pr.be_off + t.c0, 2 * kSplitN, &sm.efull[es]);
+          bulk_g2s(sm.ex[es].sc, g.Bsc + pr.be_off + t.c0, 8 * kSplitN, &sm.efull[es]);
           const int ksteps = pr.ksteps;
           const signed char* asrc = g.As + pr.a_off + (long long)(t.r0 / kSplitM) * ksteps * a_bytes;
           const signed char* bsrc = g.Bs + pr.b_off + (long long)(t.c0 / kSplitN) * ksteps * b_bytes;
@@ -484,11 +553,8 @@ __global__ void __launch_bounds__(kSplitThreads, 1) k_split(SplitArgs g) {
       if (!ok) {
         // copies still in flight write into this CTA's shared memory: wait for them (bounded)
         auto settle = [&](unsigned long long* bars, int nbars, long long issued) {
-          for (long long j = issued > nbars ? issued - nbars : 0; j < issued; ++j) {
-            void* bar = &bars[j % nbars];
-            for (long long i = 0; i < g.wait_limit; ++i)
-              if (mbar_try(bar, (unsigned)((j / nbars) & 1))) break;
-          }
+          for (long long j = issued > nbars ? issued - nbars : 0; j < issued; ++j)
+            split_settle(&bars[j % nbars], (unsigned)((j / nbars) & 1), g);
         };
         settle(sm.full, kSplitStages, n);
         settle(sm.efull, kExpSlots, q);
@@ -518,6 +584,7 @@ __global__ void __launch_bounds__(kSplitThreads, 1) k_split(SplitArgs g) {
             const signed char* b = sm.stage[st] + a_bytes;
             // A slice t times B slices 1..S+1-t in one MMA: the products land in TMEM groups
             // g = t+1 .. S+1, i.e. columns from (t-1)*32 on; t = 1 writes every group first.
+#pragma unroll
             for (int t = 1; t <= S; ++t) {
               const int nn = kSplitN * (S + 1 - t);
               umma_i8(dbase + (unsigned)((t - 1) * kSplitN), umma_desc(a + (t - 1) * kAChunk), umma_desc(b),
@@ -531,8 +598,7 @@ __global__ void __launch_bounds__(kSplitThreads, 1) k_split(SplitArgs g) {
       }
       // drain: every MMA issued above has finished before TMEM is released (bounded)
       umma_commit(&sm.drain);
-      for (long long i = 0; i < g.wait_limit; ++i)
-        if (mbar_try(&sm.drain, 0)) break;
+      split_settle(&sm.drain, 0, g);
     }
     __syncwarp();
   } else {
@@ -576,23 +642,72 @@ __global__ void __launch_bounds__(kSplitThreads, 1) k_split(SplitArgs g) {
           ok = false;
           break;
         }
-        const int er = sm.ex[es].ea[row];
-        int fe[8];
-#pragma unroll
-        for (int j = 0; j < 8; ++j) fe[j] = sm.ex[es].eb[cq * 8 + j];
-        fence_proxy_async_smem();  // as for the tile slot
-        __syncwarp();
-        if (lane == 0) mbar_arrive(&sm.eempty[es]);  // the exponents are in registers
+        // the slot's exponents and column scales are read where they are used; the slot is
+        // released after the pair's arithmetic (the ring is four deep)
+        const SplitExpSlot& ex = sm.ex[es];
+        const double* sc = &ex.sc[cq * 8];
+        const short* fe = &ex.eb[cq * 8];
+        const int er = ex.ea[row];
+        auto release_exp = [&]() {
+          fence_proxy_async_smem();  // as for the tile slot
+          __syncwarp();
+          if (lane == 0) mbar_arrive(&sm.eempty[es]);
+        };
         tc_fence_after();
-        // Per pair, element (r, c) = 2^(e_r + f_c) * sum_{g=2..S+1} 2^(-7g) P_g.  The INT32
-        // groups are combined exactly in int64 three at a time (P_g 2^14 + P_{g+1} 2^7 +
-        // P_{g+2} < 2^46), each triple is converted once and weighted by an exact power of
-        // two (smallest weights first), and the scale and the accumulation are one FMA.
-        double part[8];
+        const unsigned tb = tmem + tlane + (unsigned)(buf * kBufCols + cq * 8);
+        auto release_set = [&]() {
+          // the groups are in registers: the accumulator set may be overwritten
+          tc_fence_before();
+          __syncwarp();
+          if (lane == 0) mbar_arrive(&sm.tempty[buf]);
+        };
+        if (!warp_live) {
+          release_set();
+          release_exp();
+          continue;
+        }
+        if constexpr (Narrow) {
+          // ---- narrow: NX 32-bit sums, one conversion each
+          constexpr int NX = narrow_nx(S);
+          int X[NX][8];
+          narrow_load<S, 0, (S < 4 ? S : 4)>(tb, X);
+          if constexpr (S > 4) narrow_load<S, 4, S>(tb, X);
+          release_set();
+          constexpr double kM = 4503601774854144.0;  // 2^52 + 2^31: the conversion's offset
+          if (!general) {
+            // the row scale folded into the weights: W_k = 2^(e_r - 14k - 21) (exact, normal)
+            double W[NX];
 #pragma unroll
-        for (int j = 0; j < 8; ++j) part[j] = 0.0;
-        if (warp_live) {
-          const unsigned tb = tmem + tlane + (unsigned)(buf * kBufCols + cq * 8);
+            for (int k = 0; k < NX; ++k) W[k] = pow2(er + narrow_wexp(S, k));
+            const double mlast = -kM * W[NX - 1];
+#pragma unroll
+            for (int j = 0; j < 8; ++j) {
+              // smallest weight first; the first product is exact: (2^52 + 2^31 + X) W - (2^52 + 2^31) W
+              double part = fma(__hiloint2double(0x43300000, X[NX - 1][j] ^ (int)0x80000000), W[NX - 1], mlast);
+#pragma unroll
+              for (int k = NX - 2; k >= 0; --k)
+                part = fma(__hiloint2double(0x43300000, X[k][j] ^ (int)0x80000000) - kM, W[k], part);
+              acc[j] = fma(part, sc[j], acc[j]);
+            }
+          } else {
+#pragma unroll
+            for (int j = 0; j < 8; ++j) {
+              double part = 0.0;
+#pragma unroll
+              for (int k = NX - 1; k >= 0; --k)
+                part = fma(__hiloint2double(0x43300000, X[k][j] ^ (int)0x80000000) - kM, pow2(narrow_wexp(S, k)),
+                           part);
+              const int e = er + fe[j];
+              acc[j] = (e >= -1022 && e <= 1023) ? fma(part, pow2(e), acc[j]) : acc[j] + scalbn(part, e);
+            }
+          }
+        } else {
+          // ---- wide: the INT32 groups are combined exactly in int64 three at a time
+          // (P_g 2^14 + P_g+1 2^7 + P_g+2 < 2^46), each triple converted once and weighted by
+          // an exact power of two (smallest weights first)
+          double part[8];
+#pragma unroll
+          for (int j = 0; j < 8; ++j) part[j] = 0.0;
 #pragma unroll
           for (int c = (kMaxSlices - 1) / 3; c >= 0; --c) {
             const int g0 = 3 * c;
@@ -603,66 +718,31 @@ __global__ void __launch_bounds__(kSplitThreads, 1) k_split(SplitArgs g) {
             for (int i = 0; i < 3; ++i)
               if (i < len) tmem_ld8(tb + (unsigned)((g0 + i) * kSplitN), v[i]);
             tmem_wait_ld();
-            if (c == 0) {
-              // the last groups are in registers: the accumulator set may be overwritten
-              tc_fence_before();
-              __syncwarp();
-              if (lane == 0) mbar_arrive(&sm.tempty[buf]);
-            }
+            if (c == 0) release_set();
             // the triple's lowest group has weight 2^(-7(g0 + len - 1)) relative to group 2
             const double w = pow2(-7 * (g0 + len - 1));
-            if constexpr (Narrow) {
-              // P_g 2^7 + P_{g+1} < 2^31: the first two groups of the triple in 32 bits, the
-              // third on its own (smallest weight first)
 #pragma unroll
-              for (int j = 0; j < 8; ++j) {
-                if (len == 1) {
-                  part[j] = fma(i32_to_d((int)v[0][j]), w, part[j]);
-                } else {
-                  const int x01 = (int)v[0][j] * 128 + (int)v[1][j];
-                  if (len == 2) {
-                    part[j] = fma(i32_to_d(x01), w, part[j]);
-                  } else {
-                    part[j] = fma(i32_to_d((int)v[2][j]), w, part[j]);
-                    part[j] = fma(i32_to_d(x01), w * 128.0, part[j]);
-                  }
-                }
-              }
-            } else {
-#pragma unroll
-              for (int j = 0; j < 8; ++j) {
-                long long x = (int)v[0][j];
-                if (len > 1) x = x * 128 + (int)v[1][j];
-                if (len > 2) x = x * 128 + (int)v[2][j];
-                part[j] = fma(i2d(x), w, part[j]);
-              }
+            for (int j = 0; j < 8; ++j) {
+              long long x = (int)v[0][j];
+              if (len > 1) x = x * 128 + (int)v[1][j];
+              if (len > 2) x = x * 128 + (int)v[2][j];
+              part[j] = fma(i2d(x), w, part[j]);
             }
           }
-        }
-        if (!warp_live) {
-          tc_fence_before();
-          __syncwarp();
-          if (lane == 0) mbar_arrive(&sm.tempty[buf]);
-        }
-        if (warp_live) {
-          // 2^(e_r + f_c - 14) as a product of two exact powers of two when both factors and
-          // the product are normal (the common case, decided once per pair and thread);
-          // otherwise each element is scaled on its own (subnormal results round once)
-          bool normal = er >= -500 && er <= 500;
-#pragma unroll
-          for (int j = 0; j < 8; ++j) normal = normal && fe[j] >= -500 && fe[j] <= 500;
-          if (normal) {
+          if (!general) {
+            // part * 2^(e_r - 14) is exact (normal) and sc[j] = 2^(f_c): one rounding
             const double sr = pow2(er - 14);
 #pragma unroll
-            for (int j = 0; j < 8; ++j) acc[j] = fma(part[j], sr * pow2(fe[j]), acc[j]);
+            for (int j = 0; j < 8; ++j) acc[j] = fma(part[j] * sr, sc[j], acc[j]);
           } else {
 #pragma unroll
             for (int j = 0; j < 8; ++j) {
-              const int k = er + fe[j] - 14;
-              acc[j] = (k >= -1022 && k <= 1023) ? fma(part[j], pow2(k), acc[j]) : acc[j] + scalbn(part[j], k);
+              const int e = er + fe[j] - 14;
+              acc[j] = (e >= -1022 && e <= 1023) ? fma(part[j], pow2(e), acc[j]) : acc[j] + scalbn(part[j], e);
             }
           }
         }
+        release_exp();
       }
       if (!ok) break;
       if (row_in) {
@@ -739,6 +819,7 @@ void split_layout(sht_plan* p, int S, cudaStream_t s) {
   p->sp_b = PoolBuf(pool, std::max(bt, 16LL), s);
   p->sp_ae = PoolBuf(pool, std::max(aet, 1LL) * 2, s);
   p->sp_be = PoolBuf(pool, std::max(bet, 1LL) * 2, s);
+  p->sp_bsc = PoolBuf(pool, std::max(bet, 1LL) * 8, s);
   p->sp_meta = PoolBuf(pool, meta.size() * 8, s);
   long long* dm = p->sp_meta.as<long long>();
   p->sp_aoff = dm;
@@ -858,20 +939,22 @@ void split_slice(sht_plan* p, double alpha, cudaStream_t s) {
   const int S = p->split_slices;
   uint64_t ab;
   std::memcpy(&ab, &alpha, 8);
+  // the execute's flag words start clear (the slicer sets them)
+  SHT_CUDA(cudaMemsetAsync(p->sp_err, 0, 8, s));
   if (ab != 0) {
     const long long cap = (long long)p->ctx->num_sms * 16;
     if (p->sp_naitems)
       k_slice<<<(int)std::min((p->sp_naitems + 7) / 8, cap), 256, 0, s>>>(
           p->A->d_data.as<double>(), p->A->d_offsets.as<long long>(), p->A->d_dims.as<int>(), p->A->order,
           modes_of(p->maps.rowA), modes_of(p->maps.colA), p->sp_aoff, p->sp_aeoff,
-          p->sp_a.as<signed char>(), p->sp_ae.as<short>(), alpha, S, kSplitM, p->sp_aistart,
-          p->A->nblocks, p->sp_naitems, p->sp_err + 1);
+          p->sp_a.as<signed char>(), p->sp_ae.as<short>(), nullptr, kExpLoA, kExpHiA, alpha, S, kSplitM,
+          p->sp_aistart, p->A->nblocks, p->sp_naitems, p->sp_err);
     if (p->sp_nbitems)
       k_slice<<<(int)std::min((p->sp_nbitems + 7) / 8, cap), 256, 0, s>>>(
           p->B->d_data.as<double>(), p->B->d_offsets.as<long long>(), p->B->d_dims.as<int>(), p->B->order,
           modes_of(p->maps.colB), modes_of(p->maps.rowB), p->sp_boff, p->sp_beoff,
-          p->sp_b.as<signed char>(), p->sp_be.as<short>(), 1.0, S, kSplitN, p->sp_bistart, p->B->nblocks,
-          p->sp_nbitems, p->sp_err + 1);
+          p->sp_b.as<signed char>(), p->sp_be.as<short>(), p->sp_bsc.as<double>(), kExpLoB, kExpHiB, 1.0, S,
+          kSplitN, p->sp_bistart, p->B->nblocks, p->sp_nbitems, p->sp_err);
     SHT_CUDA(cudaGetLastError());
   }
 }
@@ -891,18 +974,24 @@ void split_launch(sht_plan* p, const SparseArgs& sa, cudaStream_t s) {
   g.Ae = p->sp_ae.as<short>();
   g.Bs = p->sp_b.as<signed char>();
   g.Be = p->sp_be.as<short>();
+  g.Bsc = p->sp_bsc.as<double>();
   g.C = sa.C;
   g.rowtab = p->sp_rowtab.as<int>();
   g.coltab = p->sp_coltab.as<int>();
   g.items = p->sp_items.as<SplitItem>();
   g.prs = p->sp_pairs.as<SplitPair>();
   g.nwork = (int)((bb == one) ? p->bwork_touched : p->bwork);
-  g.err = p->sp_err;
-  g.wait_limit = 1LL << 22;
+  g.flags = p->sp_err;
+  g.err = ctx_error_word(p->ctx);
+  g.wait_limit = p->ctx->wait_limit > 0 ? p->ctx->wait_limit : (1LL << 22);
+  g.drain_limit = 1LL << 26;
   if (g.nwork <= 0) return;
   const int grid = (int)std::min<long long>(split_grid(p->ctx), g.nwork);
   kSplitKernels[split_narrow(p, S) ? 1 : 0][S - 1]<<<grid, kSplitThreads, kSplitSmemLaunch, s>>>(g);
   SHT_CUDA(cudaGetLastError());
+  // an operand held a non-finite value (the slicer's flag): the tensor-core kernel returned at
+  // once and the FP64 tiles compute the execute, with IEEE propagation as in the FP64 forms
+  fallback_tiles_if(sa, p->d_bwork.as<int4>(), g.nwork, p->sp_err + kFlagNonFinite, p->ctx->num_sms * 4, s);
 }
 
 // ------------------------------------------------------------------ INT8 tensor-core peak
@@ -969,15 +1058,6 @@ double measure_int8_tops(sht_ctx* ctx) {
   cudaEventDestroy(e1);
   if (status) fail(SHT_ERR_TIMEOUT, "INT8 peak probe: a bounded wait on the tensor cores expired");
   return best;
-}
-
-// error words of the last split execute: [0] status from bounded waits, [1] non-finite input
-void split_check(sht_plan* p, cudaStream_t s) {
-  int e[2] = {0, 0};
-  SHT_CUDA(cudaMemcpyAsync(e, p->sp_err, 8, cudaMemcpyDeviceToHost, s));
-  SHT_CUDA(cudaStreamSynchronize(s));
-  if (e[0]) fail((sht_status)e[0], "split-precision kernel: a bounded wait on the tensor cores expired");
-  if (e[1]) fail(SHT_ERR_UNSUPPORTED, "split-precision mode needs finite inputs");
 }
 
 }  // namespace sht

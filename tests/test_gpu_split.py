@@ -80,13 +80,64 @@ def test_split_slice_count_tradeoff(ctx):
     assert errs[7] <= REL_TOL and errs[4] > errs[7]
 
 
-def test_split_rejects_non_finite(ctx):
+def test_split_non_finite_inputs_follow_the_fp64_forms(ctx):
+    # an operand with Inf and NaN: the execute is computed by the FP64 tiles, so the result is
+    # the plain form's, bit for bit (IEEE propagation), and the call does not fail
+    from tests.bits import bits_equal
     w = W.c0(seed=6, nblocks=4, p=0.6)
     w.A.data[3] = np.inf
+    w.B.data[5] = np.nan
+    A, B = dev(ctx, w.A), dev(ctx, w.B)
+    Cs, Cp = dev(ctx, w.C), dev(ctx, w.C)
+    sht.contract(ctx, w.expr, 1.0, A, B, 0.0, Cs, mode=sht.Mode.SPLIT)
+    sht.contract(ctx, w.expr, 1.0, A, B, 0.0, Cp, mode=sht.Mode.PLAIN_FP64)
+    ctx.stream_sync()
+    got, want = Cs.download(), Cp.download()
+    assert np.isnan(got).any() and np.isinf(got).any()
+    assert bits_equal(got, want)
+    # the same plan with finite data again takes the tensor-core path
+    w2 = W.c0(seed=6, nblocks=4, p=0.6)
+    A.upload(w2.A.data)
+    B.upload(w2.B.data)
+    err, mx, _ = run_split(ctx, w2)
+    assert err <= REL_TOL, (err, mx)
+
+
+def test_split_queued_back_to_back(ctx):
+    # two split contractions queued on one stream with no host wait between them (the second
+    # accumulates into the first's output), then one synchronization: both as the oracle
+    import torch
+    w = W.c1(seed=13, scale=0.25, occupancy=0.4)
+    A, B, C1, C2 = dev(ctx, w.A), dev(ctx, w.B), dev(ctx, w.C), dev(ctx, w.C)
+    s = torch.cuda.Stream()
+    sht.contract(ctx, w.expr, 1.0, A, B, 0.0, C1, mode=sht.Mode.SPLIT, stream=s)
+    sht.contract(ctx, w.expr, 0.5, A, B, 0.0, C2, mode=sht.Mode.SPLIT, stream=s)
+    sht.contract(ctx, w.expr, 1.0, A, B, 2.0, C1, mode=sht.Mode.SPLIT, stream=s)
+    ctx.stream_sync(s)
+    want = oracle.contract(w.expr, 1.0, host(w.A), host(w.B), 0.0, host(w.C))
+    want3 = oracle.contract(w.expr, 1.0, host(w.A), host(w.B), 2.0, want.C)
+    for C, ref in ((C1, want3.C.data), (C2, 0.5 * want.C.data)):
+        got = C.download()
+        assert np.linalg.norm(got - ref) <= REL_TOL * np.linalg.norm(ref)
+
+
+def test_split_bounded_wait_reports_timeout(ctx):
+    # a one-poll wait limit makes the pipeline waits run out: the launch stops (its in-flight
+    # copies and MMAs drained under their own bound), the context records SHT_ERR_TIMEOUT, the
+    # stream sync reports it once, and the context keeps working afterwards
+    w = W.c1(seed=14, scale=0.25, occupancy=0.4)
     A, B, C = dev(ctx, w.A), dev(ctx, w.B), dev(ctx, w.C)
-    with pytest.raises(sht.ShtError) as ei:
+    ctx.set_wait_limit(1)
+    try:
         sht.contract(ctx, w.expr, 1.0, A, B, 0.0, C, mode=sht.Mode.SPLIT)
-    assert ei.value.status == sht.Status.ERR_UNSUPPORTED
+        with pytest.raises(sht.ShtError) as ei:
+            ctx.stream_sync()
+        assert ei.value.status == sht.Status.ERR_TIMEOUT
+    finally:
+        ctx.set_wait_limit(0)
+    ctx.stream_sync()  # reported once
+    err, mx, _ = run_split(ctx, w)
+    assert err <= REL_TOL, (err, mx)
 
 
 def test_compare_entry_point(ctx):
@@ -117,12 +168,17 @@ def per_block_errors(ctx, w):
     return out
 
 
-def test_split_extreme_exponents(ctx):
-    # row / column exponents far outside [-480, 480] and subnormal products take the general
-    # conversion and scaling; in-range ones the scale-folded conversion; same launch
+@pytest.mark.parametrize("scales", [((1e-150, 1.0, 1e150), (1e150, 1e-160, 1.0)),
+                                    ((1e-280, 1.0, 1e280), (1e10, 1e-30, 1.0)),
+                                    ((1.0, 2.0, 3.0), (1e-310, 1e300, 1.0))])
+def test_split_extreme_exponents(ctx, scales):
+    # far-apart row / column exponents and subnormal products.  The first set stays inside the
+    # scale-folded range (A rows 2^-900 .. 2^960, B columns normal); in the second an A row
+    # maximum near 1e-280 and in the third a subnormal B column fall outside it, so the launch
+    # scales every element on its own
     rng = np.random.default_rng(11)
     bi, bk, bj = [8, 12, 16], [20, 40], [10, 24, 6]
-    sa, sb = np.array([1e-150, 1.0, 1e150]), np.array([1e150, 1e-160, 1.0])
+    sa, sb = np.array(scales[0]), np.array(scales[1])
     A = W.build_tensor(rng, [bi, bk], lambda c: np.ones(len(c[0]), bool), lambda c: sa[c[0]], "normal")
     B = W.build_tensor(rng, [bk, bj], lambda c: np.ones(len(c[0]), bool), lambda c: sb[c[1]], "normal")
     w = W.Workload("extreme", "ik, kj -> ij", A, B, W.empty_tensor([bi, bj]))
@@ -135,8 +191,8 @@ def test_split_extreme_exponents(ctx):
 
 
 def test_split_long_contracted_extent(ctx):
-    # K = 9728: seven INT32 groups of up to 7 * 127^2 * K no longer fit the scale-folded
-    # conversion of the low part (|L| >= 2^51 possible), so the launch converts generally
+    # K = 9728: the INT32 group sums reach 7 * 127^2 * K > 2^23, beyond the 32-bit pairing of the
+    # narrow reassembly, so the launch combines the groups in int64 (the wide instance)
     rng = np.random.default_rng(12)
     bi, bk, bj = [8, 24], [9728], [16, 8]
     A = W.build_tensor(rng, [bi, bk], lambda c: np.ones(len(c[0]), bool), None, "normal")
