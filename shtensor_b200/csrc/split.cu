@@ -75,23 +75,26 @@ __host__ __device__ __forceinline__ int slab_offset(int r, int k) {
 constexpr int kFlagNonFinite = 0, kFlagGeneralExp = 1;
 constexpr int kExpLoA = -900, kExpHiA = 960, kExpLoB = -1022, kExpHiB = 1023;
 
-// One warp per item of 32 rows of one block (lane = row; items are numbered block after block,
-// istart[b] the first item of block b): the row maximum gives the row's
-// exponent (rows padded up to the tile height R get 0), then the S int8 slices of the row
-// go out in tile order: out[((tile * ksteps + ks) * S + t) * R * 32 + slab_offset(row % R, k)].
+// One 128-thread CTA per item of 32 rows of one block (items are numbered block after block,
+// istart[b] the first item of block b).  Lane = row; warp w takes the 16-wide k-chunks w, w+4,
+// ... of the row (a warp's load of one k is 32 consecutive rows of a column-major block).  The
+// first chunk of each warp stays in registers (every chunk when K <= 64); the row maximum is
+// reduced over the four warps in shared memory and gives the row's exponent (rows padded up to
+// the tile height R get 0); then every chunk is cut into its S int8 slices, packed four bytes
+// to a register and stored as one 16-byte word per slice, in tile order:
+//   out[((tile * ksteps + ks) * S + t) * R * 32 + slab_offset(row % R, k)].
 // Rows past the block and k past K are zero.  With pscale set (B columns), the row's scale 2^e
 // is also written as a double (0 when e is outside [elo, ehi]).
-__global__ void __launch_bounds__(256) k_slice(const double* __restrict__ src, const long long* __restrict__ src_off,
-                                               const int* __restrict__ dims, int order, ModeMap fm, ModeMap km,
-                                               const long long* __restrict__ out_off,
-                                               const long long* __restrict__ exp_off, signed char* __restrict__ out,
-                                               short* __restrict__ expo, double* __restrict__ pscale, int elo, int ehi,
-                                               double scale, int S, int R,
-                                               const long long* __restrict__ istart, long long nblocks,
-                                               long long nitems, int* __restrict__ flags) {
-  const int lane = threadIdx.x & 31;
-  const long long nwarps = (long long)gridDim.x * (blockDim.x >> 5);
-  for (long long it = blockIdx.x * (long long)(blockDim.x >> 5) + (threadIdx.x >> 5); it < nitems; it += nwarps) {
+constexpr int kSliceWarps = 4;
+__global__ void __launch_bounds__(kSliceWarps * 32, 4) k_slice(
+    const double* __restrict__ src, const long long* __restrict__ src_off, const int* __restrict__ dims, int order,
+    ModeMap fm, ModeMap km, const long long* __restrict__ out_off, const long long* __restrict__ exp_off,
+    signed char* __restrict__ out, short* __restrict__ expo, double* __restrict__ pscale, int elo, int ehi,
+    double scale, int S, int R, const long long* __restrict__ istart, long long nblocks, long long nitems,
+    int* __restrict__ flags) {
+  __shared__ double wmax[kSliceWarps][32];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  for (long long it = blockIdx.x; it < nitems; it += gridDim.x) {
     // the block holding item it: the last block whose first item is <= it
     long long lo = 0, hi = nblocks;
     while (hi - lo > 1) {
@@ -107,7 +110,7 @@ __global__ void __launch_bounds__(256) k_slice(const double* __restrict__ src, c
     for (int t = 0; t < fm.n; ++t) m *= d[fm.x[t]];
     for (int t = 0; t < km.n; ++t) K *= d[km.x[t]];
     const int Kp = (K + kSplitK - 1) / kSplitK * kSplitK;
-    const int ksteps = Kp / kSplitK;
+    const int ksteps = Kp / kSplitK, nchunks = Kp / 16;
     auto offset = [&](const ModeMap& mm, int idx) {
       int off = 0;
       for (int t = 0; t < mm.n; ++t) {
@@ -124,32 +127,64 @@ __global__ void __launch_bounds__(256) k_slice(const double* __restrict__ src, c
     const double* s = src + src_off[b];
     const bool live = r < m;
     const int fr = live ? offset(fm, r) : 0;
-    // pass 1: the row exponent (|v| / 2^e < 1)
+    auto load_chunk = [&](int c, double (&v)[16]) {
+#pragma unroll
+      for (int j = 0; j < 16; ++j) {
+        const int k = c * 16 + j;
+        v[j] = (live && k < K) ? __dmul_rn(s[fr + koff(k)], scale) : 0.0;
+      }
+    };
+    // pass over this warp's chunks: the first stays in registers
+    double v0[16];
     double mx = 0.0;
-    if (live) {
-      for (int k = 0; k < K; ++k) {
-        const double v = __dmul_rn(s[fr + koff(k)], scale);
-        if (!isfinite(v)) atomicExch(&flags[kFlagNonFinite], 1);
-        mx = fmax(mx, fabs(v));
+    bool finite = true;
+    if (warp < nchunks) {
+      load_chunk(warp, v0);
+#pragma unroll
+      for (int j = 0; j < 16; ++j) {
+        finite = finite && isfinite(v0[j]);
+        mx = fmax(mx, fabs(v0[j]));
       }
     }
+    for (int c = warp + kSliceWarps; c < nchunks; c += kSliceWarps) {
+      double v[16];
+      load_chunk(c, v);
+#pragma unroll
+      for (int j = 0; j < 16; ++j) {
+        finite = finite && isfinite(v[j]);
+        mx = fmax(mx, fabs(v[j]));
+      }
+    }
+    if (!finite) atomicExch(&flags[kFlagNonFinite], 1);
+    wmax[warp][lane] = mx;
+    __syncthreads();
+    mx = fmax(fmax(wmax[0][lane], wmax[1][lane]), fmax(wmax[2][lane], wmax[3][lane]));
+    __syncthreads();  // wmax is rewritten by the next item
     int e = 0;
     if (mx > 0.0) frexp(mx, &e);
-    expo[exp_off[b] + r] = (short)e;
-    const bool in_range = e >= elo && e <= ehi;
-    if (!in_range) atomicExch(&flags[kFlagGeneralExp], 1);
-    if (pscale) pscale[exp_off[b] + r] = in_range ? ldexp(1.0, e) : 0.0;
-    // pass 2: 16 k at a time; the S slices are packed four bytes to a register and stored
-    // as one 16-byte word each
+    if (warp == 0) {
+      expo[exp_off[b] + r] = (short)e;
+      const bool in_range = e >= elo && e <= ehi;
+      if (!in_range) atomicExch(&flags[kFlagGeneralExp], 1);
+      if (pscale) pscale[exp_off[b] + r] = in_range ? ldexp(1.0, e) : 0.0;
+    }
+    // slices of every chunk of this warp: 16 k at a time, the S slices packed four bytes to a
+    // register and stored as one 16-byte word each
     signed char* o = out + out_off[b] + (long long)(r / R) * ksteps * S * R * kSplitK;
-    for (int q = 0; q < Kp / 16; ++q) {
+    for (int c = warp; c < nchunks; c += kSliceWarps) {
+      double v[16];
+      if (c == warp) {
+#pragma unroll
+        for (int j = 0; j < 16; ++j) v[j] = v0[j];
+      } else {
+        load_chunk(c, v);
+      }
       unsigned w[kMaxSlices][4];
 #pragma unroll
       for (int t = 0; t < kMaxSlices; ++t) w[t][0] = w[t][1] = w[t][2] = w[t][3] = 0u;
 #pragma unroll
       for (int j = 0; j < 16; ++j) {
-        const int k = q * 16 + j;
-        double x = (live && k < K) ? scalbn(__dmul_rn(s[fr + koff(k)], scale), -e) : 0.0;
+        double x = scalbn(v[j], -e);
 #pragma unroll
         for (int t = 0; t < kMaxSlices; ++t) {
           const double y = x * 128.0;
@@ -158,7 +193,7 @@ __global__ void __launch_bounds__(256) k_slice(const double* __restrict__ src, c
           x = y - tr;
         }
       }
-      const long long base = (long long)(q / 2) * S * R * kSplitK + slab_offset(r % R, (q & 1) * 16);
+      const long long base = (long long)(c / 2) * S * R * kSplitK + slab_offset(r % R, (c & 1) * 16);
 #pragma unroll
       for (int t = 0; t < kMaxSlices; ++t)
         if (t < S)
@@ -942,15 +977,15 @@ void split_slice(sht_plan* p, double alpha, cudaStream_t s) {
   // the execute's flag words start clear (the slicer sets them)
   SHT_CUDA(cudaMemsetAsync(p->sp_err, 0, 8, s));
   if (ab != 0) {
-    const long long cap = (long long)p->ctx->num_sms * 16;
+    const long long cap = (long long)p->ctx->num_sms * 32;
     if (p->sp_naitems)
-      k_slice<<<(int)std::min((p->sp_naitems + 7) / 8, cap), 256, 0, s>>>(
+      k_slice<<<(int)std::min(p->sp_naitems, cap), kSliceWarps * 32, 0, s>>>(
           p->A->d_data.as<double>(), p->A->d_offsets.as<long long>(), p->A->d_dims.as<int>(), p->A->order,
           modes_of(p->maps.rowA), modes_of(p->maps.colA), p->sp_aoff, p->sp_aeoff,
           p->sp_a.as<signed char>(), p->sp_ae.as<short>(), nullptr, kExpLoA, kExpHiA, alpha, S, kSplitM,
           p->sp_aistart, p->A->nblocks, p->sp_naitems, p->sp_err);
     if (p->sp_nbitems)
-      k_slice<<<(int)std::min((p->sp_nbitems + 7) / 8, cap), 256, 0, s>>>(
+      k_slice<<<(int)std::min(p->sp_nbitems, cap), kSliceWarps * 32, 0, s>>>(
           p->B->d_data.as<double>(), p->B->d_offsets.as<long long>(), p->B->d_dims.as<int>(), p->B->order,
           modes_of(p->maps.colB), modes_of(p->maps.rowB), p->sp_boff, p->sp_beoff,
           p->sp_b.as<signed char>(), p->sp_be.as<short>(), p->sp_bsc.as<double>(), kExpLoB, kExpHiB, 1.0, S,
