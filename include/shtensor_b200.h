@@ -198,8 +198,11 @@ sht_status sht_measure_peak(sht_ctx* ctx, int which, double* value);
 
 /* ---- serving loop (no reference counterpart: shtensor has no request loop) ----
  * A server owns one host thread and its own CUDA streams.  Requests are block-sparse
- * contractions over device-resident tensors, computed in the batched FP64 form (the result
- * bits equal sht_contract with SHT_MODE_BATCHED_FP64 or SHT_MODE_PLAIN_FP64 run alone).
+ * contractions over device-resident tensors, computed in the server's form: the batched FP64
+ * form (the result bits equal sht_contract with SHT_MODE_BATCHED_FP64 or SHT_MODE_PLAIN_FP64
+ * run alone), or the split-precision form (the result bits equal sht_contract with
+ * SHT_MODE_SPLIT run alone; a request whose operands hold a non-finite value or an exponent
+ * outside the split kernel's scale-folded range is served in the batched FP64 form).
  * Continuous batching: a request that arrives while others run is planned at once (by one of
  * several planner threads) if a slot is free and the pool has room, and joins the next
  * persistent launch together with every other planned request; up to two launches are
@@ -219,8 +222,11 @@ typedef struct {
   int max_batch;         /* requests fused into one launch (0 = 32) */
   size_t reserve_bytes;  /* pool bytes that admission leaves free (0 = none) */
   int planners;          /* planner threads, each with its own stream (0 = 8) */
-  int ctas_per_sm;       /* persistent CTAs per SM of a serving launch (0 = the most that fit
-                            minus one, leaving room for planning kernels) */
+  int ctas_per_sm;       /* persistent CTAs per SM of a batched serving launch (0 = the most
+                            that fit minus one, leaving room for planning kernels) */
+  int mode;              /* 0 or SHT_MODE_BATCHED_FP64: batched FP64; SHT_MODE_SPLIT: split
+                            precision.  One launch holds requests of one form (and, in split
+                            form, one slice count and reassembly instance). */
 } sht_server_config;
 
 typedef struct {
@@ -232,6 +238,7 @@ typedef struct {
   double run_ms;         /* launch -> completion observed */
   double latency_ms;     /* submit -> completion observed */
   int64_t batch;         /* id of the launch that computed it (-1 if it never ran) */
+  int form;              /* the form that computed it (an sht_mode value) */
   int batch_size;        /* requests in that launch */
   int deferrals;         /* admissions put off for pool memory */
 } sht_request_report;

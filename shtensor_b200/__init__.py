@@ -73,13 +73,13 @@ class Report(C.Structure):
 
 class ServerConfig(C.Structure):
     _fields_ = [("max_active", C.c_int), ("max_batch", C.c_int), ("reserve_bytes", C.c_size_t),
-                ("planners", C.c_int), ("ctas_per_sm", C.c_int)]
+                ("planners", C.c_int), ("ctas_per_sm", C.c_int), ("mode", C.c_int)]
 
 
 class RequestReport(C.Structure):
     _fields_ = [("status", C.c_int), ("npairs", C.c_int64), ("flops", C.c_double), ("queue_ms", C.c_double),
                 ("plan_ms", C.c_double), ("run_ms", C.c_double), ("latency_ms", C.c_double),
-                ("batch", C.c_int64), ("batch_size", C.c_int), ("deferrals", C.c_int)]
+                ("batch", C.c_int64), ("form", C.c_int), ("batch_size", C.c_int), ("deferrals", C.c_int)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}
@@ -490,14 +490,18 @@ class Server:
     """Serving loop: continuous batching of contractions over device-resident tensors.
 
     ``submit`` queues ``C = beta*C + alpha*contract(expr, A, B)`` and returns a request id;
-    ``wait`` returns the request's report (and raises if the request failed).  Results equal
-    :func:`contract` in ``Mode.BATCHED_FP64`` (and ``Mode.PLAIN_FP64``) bit for bit.  The
+    ``wait`` returns the request's report (and raises if the request failed).  With
+    ``mode=Mode.BATCHED_FP64`` (the default) results equal :func:`contract` in
+    ``Mode.BATCHED_FP64`` (and ``Mode.PLAIN_FP64``) bit for bit; with ``mode=Mode.SPLIT`` they
+    equal :func:`contract` in ``Mode.SPLIT`` (a request with non-finite values or out-of-range
+    exponents is served in the batched FP64 form; its report's ``form`` says which).  The
     tensors of a request must stay alive and unmodified until it has finished.
     """
 
     def __init__(self, ctx: Context, max_active: int = 0, max_batch: int = 0, reserve_bytes: int = 0,
-                 planners: int = 0, ctas_per_sm: int = 0):
-        cfg = ServerConfig(max_active, max_batch, reserve_bytes, planners, ctas_per_sm)
+                 planners: int = 0, ctas_per_sm: int = 0, mode: "Mode" = None):
+        cfg = ServerConfig(max_active, max_batch, reserve_bytes, planners, ctas_per_sm,
+                           int(mode) if mode is not None else 0)
         h = _P()
         _check(lib().sht_server_create(ctx.handle, C.byref(cfg), C.byref(h)))
         self._h = h

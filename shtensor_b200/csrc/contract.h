@@ -119,6 +119,14 @@ void split_launch(sht_plan* p, const SparseArgs& sa, cudaStream_t s);
 void fallback_tiles_if(const SparseArgs& g, const int4* work, long long nwork, const int* flag, int grid,
                        cudaStream_t s);
 int split_slices_default();
+// Serving: requests of one launch share the kind (slice count and reassembly instance); the
+// host buffer holds split_desc_bytes() per request; the flags are read after the slicer (a
+// synchronization of s) and must be clear for a request to join a split launch.
+int split_kind(const sht_plan* p);
+size_t split_desc_bytes();
+bool split_flags_clear(sht_plan* p, cudaStream_t s);
+long long split_multi_launch(sht_ctx* ctx, const std::vector<sht_plan*>& plans, const std::vector<SparseArgs>& args,
+                             void* host_descs, PoolBuf& descs, cudaStream_t s);
 void matform_execute(sht_plan* p, double alpha, cudaStream_t s);
 void block_dims_sizes(const sht_tensor* t, const long long* ids, long long n, int* dims, long long* sizes,
                       cudaStream_t s);

@@ -1,4 +1,5 @@
-// server.cpp -- serving loop: continuous batching of block-sparse contractions on one GPU.
+// server.cpp -- serving loop: continuous batching of block-sparse contractions on one GPU,
+// in the batched FP64 or the split-precision form.
 //
 // shtensor itself has no request loop; this is the library's own.  A server runs one loop
 // thread and `planners` planner threads.  A request moves through
@@ -69,6 +70,8 @@ struct Request {
   int64_t deferred_at = -1;     // retired-launch count when it was deferred
   int64_t npairs = 0;
   double flops = 0.0;
+  int form = SHT_MODE_BATCHED_FP64;  // the form it was planned in
+  int kind = -1;                     // split form: the launch kind (slice count, reassembly)
 };
 using ReqPtr = std::shared_ptr<Request>;
 
@@ -96,6 +99,7 @@ struct sht_server {
   sht_ctx* ctx = nullptr;
   std::shared_ptr<sht::DevicePool> keep;
   int max_active = 64, max_batch = 32, nplanners = 8, ctas_per_sm = 0;
+  int mode = SHT_MODE_BATCHED_FP64;  // the served form
   size_t reserve_bytes = 0;
   cudaStream_t exec_stream = nullptr;
   std::vector<cudaStream_t> plan_streams;
@@ -208,8 +212,15 @@ bool sht_server::retire() {
     const cudaError_t q = cudaEventQuery(l.done);
     if (q == cudaErrorNotReady) break;
     const Clock::time_point t = Clock::now();
-    const sht_status st = q == cudaSuccess ? SHT_OK : SHT_ERR_CUDA;
-    const std::string msg = q == cudaSuccess ? "" : std::string("serving launch failed: ") + cudaGetErrorString(q);
+    sht_status st = q == cudaSuccess ? SHT_OK : SHT_ERR_CUDA;
+    std::string msg = q == cudaSuccess ? "" : std::string("serving launch failed: ") + cudaGetErrorString(q);
+    // a split launch whose bounded wait ran out recorded it on the context's error word
+    if (st == SHT_OK) {
+      if (const int e = sht::ctx_take_error(ctx)) {
+        st = (sht_status)e;
+        msg = "serving launch failed: a bounded wait on the tensor cores expired";
+      }
+    }
     if (q != cudaSuccess) (void)cudaGetLastError();
     strace("retire launch %lld (%lld requests)", (long long)l.id, (long long)l.reqs.size());
     for (const ReqPtr& r : l.reqs) finish(r, st, msg, t);
@@ -349,10 +360,28 @@ void sht_server::planner(int index) {
     r->pstream = s;
     r->t_plan0 = Clock::now();
     try {
-      r->plan.reset(sht::plan_create(ctx, r->expr, r->A, r->B, r->C, r->eps, r->norm, SHT_MODE_BATCHED_FP64, s));
-      sht::batched_prepare(r->plan.get(), s);
-      const sht::SparseArgs g = sht::sparse_args(r->plan.get(), r->alpha, r->beta);
-      if (!g.sc.alpha_zero) sht::matform_execute(r->plan.get(), r->alpha, s);
+      bool split = false;
+      if (mode == SHT_MODE_SPLIT) {
+        // split form: pairs, C pattern, slices and records; the slicer's flags are read here (the
+        // planner synchronizes anyway), and a request they rule out is planned again in the
+        // batched FP64 form
+        r->plan.reset(sht::plan_create(ctx, r->expr, r->A, r->B, r->C, r->eps, r->norm, SHT_MODE_SPLIT, s));
+        sht::split_prepare(r->plan.get(), ctx->split_slices ? ctx->split_slices : sht::split_slices_default(), s);
+        sht::split_slice(r->plan.get(), r->alpha, s);
+        split = sht::split_flags_clear(r->plan.get(), s);
+        if (!split) r->plan.reset();
+      }
+      if (split) {
+        r->form = SHT_MODE_SPLIT;
+        r->kind = sht::split_kind(r->plan.get());
+      } else {
+        r->form = SHT_MODE_BATCHED_FP64;
+        r->kind = -1;
+        r->plan.reset(sht::plan_create(ctx, r->expr, r->A, r->B, r->C, r->eps, r->norm, SHT_MODE_BATCHED_FP64, s));
+        sht::batched_prepare(r->plan.get(), s);
+        const sht::SparseArgs g = sht::sparse_args(r->plan.get(), r->alpha, r->beta);
+        if (!g.sc.alpha_zero) sht::matform_execute(r->plan.get(), r->alpha, s);
+      }
       SHT_CUDA(cudaEventRecord(r->planned, s));
       r->npairs = r->plan->npairs;
       r->flops = sht::plan_flops(r->plan.get(), s);
@@ -377,16 +406,25 @@ void sht_server::planner(int index) {
   }
 }
 
-// Put every ready request (up to max_batch) into one persistent launch on the exec stream.
+// Put the ready requests of the oldest ready request's kind (batched FP64, or one split kind),
+// up to max_batch, into one persistent launch on the exec stream.
 bool sht_server::launch() {
   if (ready.empty() || running.size() >= 2) return false;
   const int slot = slot_busy[0] ? 1 : 0;
   auto l = std::make_unique<Launch>();
   l->id = next_launch++;
   l->slot = slot;
-  const size_t n = std::min<size_t>(ready.size(), (size_t)max_batch);
-  l->reqs.assign(ready.begin(), ready.begin() + n);
-  ready.erase(ready.begin(), ready.begin() + n);
+  const int kind = (*std::min_element(ready.begin(), ready.end(),
+                                      [](const ReqPtr& a, const ReqPtr& b) { return a->id < b->id; }))->kind;
+  for (auto it = ready.begin(); it != ready.end() && l->reqs.size() < (size_t)max_batch;) {
+    if ((*it)->kind == kind) {
+      l->reqs.push_back(*it);
+      it = ready.erase(it);
+    } else {
+      ++it;
+    }
+  }
+  const size_t n = l->reqs.size();
   const Clock::time_point t = Clock::now();
   try {
     std::vector<sht_plan*> plans;
@@ -400,8 +438,12 @@ bool sht_server::launch() {
       r->batch = l->id;
       r->batch_size = (int)n;
     }
-    const int per_sm = ctas_per_sm > 0 ? ctas_per_sm : std::max(1, sht::batched_ctas_per_sm(ctx) - 1);
-    sht::batched_multi_launch(ctx, plans, args, pinned[slot], l->descs, l->counter, per_sm, exec_stream);
+    if (kind >= 0) {
+      sht::split_multi_launch(ctx, plans, args, pinned[slot], l->descs, exec_stream);
+    } else {
+      const int per_sm = ctas_per_sm > 0 ? ctas_per_sm : std::max(1, sht::batched_ctas_per_sm(ctx) - 1);
+      sht::batched_multi_launch(ctx, plans, args, pinned[slot], l->descs, l->counter, per_sm, exec_stream);
+    }
     l->descs.use_on(exec_stream);
     l->counter.use_on(exec_stream);
     SHT_CUDA(cudaEventCreateWithFlags(&l->done, cudaEventDisableTiming));
@@ -467,6 +509,9 @@ sht_status sht_server_create(sht_ctx* ctx, const sht_server_config* cfg, sht_ser
       if (cfg->planners) s->nplanners = std::min(cfg->planners, 64);
       s->ctas_per_sm = cfg->ctas_per_sm;
       s->reserve_bytes = cfg->reserve_bytes;
+      if (cfg->mode != 0 && cfg->mode != SHT_MODE_BATCHED_FP64 && cfg->mode != SHT_MODE_SPLIT)
+        fail(SHT_ERR_INVALID, "a server serves the batched FP64 or the split-precision form");
+      s->mode = cfg->mode == SHT_MODE_SPLIT ? SHT_MODE_SPLIT : SHT_MODE_BATCHED_FP64;
     }
     SHT_CUDA(cudaSetDevice(ctx->device));
     int lo = 0, hi = 0;
@@ -485,7 +530,8 @@ sht_status sht_server_create(sht_ctx* ctx, const sht_server_config* cfg, sht_ser
         s->plan_streams.push_back(st);
       }
       SHT_CUDA(cudaStreamCreateWithPriority(&s->exec_stream, cudaStreamNonBlocking, lo));
-      for (void*& p : s->pinned) SHT_CUDA(cudaMallocHost(&p, (size_t)s->max_batch * batched_desc_bytes()));
+      for (void*& p : s->pinned)
+        SHT_CUDA(cudaMallocHost(&p, (size_t)s->max_batch * std::max(batched_desc_bytes(), split_desc_bytes())));
     } catch (...) {
       cleanup();
       throw;
@@ -569,6 +615,7 @@ sht_status sht_server_wait(sht_server* srv, int64_t request_id, double timeout_s
     rep->run_ms = r->batch >= 0 ? ms_between(r->t_launch, r->t_done) : 0.0;
     rep->latency_ms = ms_between(r->t_submit, r->t_done);
     rep->batch = r->batch;
+    rep->form = r->form;
     rep->batch_size = r->batch_size;
     rep->deferrals = r->deferrals;
   }

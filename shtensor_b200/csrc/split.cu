@@ -412,6 +412,11 @@ struct SplitArgs {
   const SplitPair* prs;    // per block pair
   int nwork;
   const int* flags;        // the execute's flag words (kFlag*)
+  // several requests in one launch (serving): their arguments, and the first global item of
+  // each (ascending); nwork is then the total.  0 for a launch of this plan alone.
+  const SplitArgs* multi;
+  const int* mfirst;
+  int nmulti;
   volatile int* err;       // the context's error word (host-mapped): SHT_ERR_TIMEOUT
   long long wait_limit;    // polls of one pipeline wait before the launch gives up
   long long drain_limit;   // polls of the waits for work already issued (copies, MMAs)
@@ -446,6 +451,21 @@ struct SplitSmem {
   unsigned tmem_base;
   int abort;
 };
+
+// The request that global item `item` belongs to and its item index there.
+__device__ __forceinline__ const SplitArgs& split_req(const SplitArgs& g, int item, int& li) {
+  if (g.nmulti == 0) {
+    li = item;
+    return g;
+  }
+  int lo = 0, hi = g.nmulti;  // the last request whose first item is <= item
+  while (hi - lo > 1) {
+    const int mid = (lo + hi) >> 1;
+    if (g.mfirst[mid] <= item) lo = mid; else hi = mid;
+  }
+  li = item - g.mfirst[lo];
+  return g.multi[lo];
+}
 
 // bounded wait that also gives up when another role raised the abort flag
 __device__ __forceinline__ bool split_wait(void* mbar, unsigned parity, volatile int* abort, const SplitArgs& g) {
@@ -507,15 +527,14 @@ __device__ __forceinline__ void narrow_load(unsigned tb, int (&X)[narrow_nx(S)][
 // is below 2^23 in magnitude (the host checks S * 127^2 * K), so groups combine two by two in
 // 32 bits and each pair converts with one integer operation and one FP64 add.
 template <int S, bool Narrow>
-__global__ void __maxnreg__(112) k_split(SplitArgs g) {
-  // an operand holds a non-finite value: the FP64 tile kernel computes this execute
-  if (g.flags[kFlagNonFinite]) return;
+__global__ void __maxnreg__(112) k_split(const __grid_constant__ SplitArgs g) {
+  // an operand holds a non-finite value: the FP64 tile kernel computes this execute (in a
+  // launch of several requests every role skips such a request's tiles alike)
+  if (g.nmulti == 0 && g.flags[kFlagNonFinite]) return;
   extern __shared__ __align__(1024) unsigned char smem_raw[];
   SplitSmem& sm = *reinterpret_cast<SplitSmem*>(smem_raw);
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   volatile int* abort = &sm.abort;
-  // some row or column exponent lies outside the scale-folded range (uniform over the launch)
-  const bool general = g.flags[kFlagGeneralExp] != 0;
 
   if (warp == 0) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&sm.tmem_base)),
@@ -555,26 +574,30 @@ __global__ void __maxnreg__(112) k_split(SplitArgs g) {
     if (lane == 0) {
       long long n = 0, q = 0, ni = 0;
       bool ok = true;
-      for (int item = blockIdx.x; ok && item < g.nwork; item += gridDim.x, ++ni) {
-        const SplitItem t = g.items[item];
+      for (int item = blockIdx.x; ok && item < g.nwork; item += gridDim.x) {
+        int li;
+        const SplitArgs& a = split_req(g, item, li);
+        if (a.flags[kFlagNonFinite]) continue;
+        const SplitItem t = a.items[li];
         const int is = (int)(ni % kTileSlots);
         if (!split_wait(&sm.iempty[is], (unsigned)(((ni / kTileSlots) & 1) ^ 1), abort, g)) { ok = false; break; }
+        ++ni;
         mbar_expect_tx(&sm.ifull[is], kTileSlotBytes);
-        bulk_g2s(&sm.tile[is].rec, g.items + item, sizeof(SplitItem), &sm.ifull[is]);
-        bulk_g2s(sm.tile[is].rowoff, g.rowtab + t.rtab, 4 * kSplitM, &sm.ifull[is]);
-        bulk_g2s(sm.tile[is].coloff, g.coltab + t.ctab, 4 * kSplitN, &sm.ifull[is]);
-        const int pe = g.alpha_zero ? t.pb : t.pe;
+        bulk_g2s(&sm.tile[is].rec, a.items + li, sizeof(SplitItem), &sm.ifull[is]);
+        bulk_g2s(sm.tile[is].rowoff, a.rowtab + t.rtab, 4 * kSplitM, &sm.ifull[is]);
+        bulk_g2s(sm.tile[is].coloff, a.coltab + t.ctab, 4 * kSplitN, &sm.ifull[is]);
+        const int pe = a.alpha_zero ? t.pb : t.pe;
         for (int p = t.pb; ok && p < pe; ++p, ++q) {
-          const SplitPair pr = g.prs[p];
+          const SplitPair pr = a.prs[p];
           const int es = (int)(q % kExpSlots);
           if (!split_wait(&sm.eempty[es], (unsigned)(((q / kExpSlots) & 1) ^ 1), abort, g)) { ok = false; break; }
           mbar_expect_tx(&sm.efull[es], kExpSlotBytes);
-          bulk_g2s(sm.ex[es].ea, g.Ae + pr.ae_off + t.r0, 2 * kSplitM, &sm.efull[es]);
-          bulk_g2s(sm.ex[es].eb, g.Be + pr.be_off + t.c0, 2 * kSplitN, &sm.efull[es]);
-          bulk_g2s(sm.ex[es].sc, g.Bsc + pr.be_off + t.c0, 8 * kSplitN, &sm.efull[es]);
+          bulk_g2s(sm.ex[es].ea, a.Ae + pr.ae_off + t.r0, 2 * kSplitM, &sm.efull[es]);
+          bulk_g2s(sm.ex[es].eb, a.Be + pr.be_off + t.c0, 2 * kSplitN, &sm.efull[es]);
+          bulk_g2s(sm.ex[es].sc, a.Bsc + pr.be_off + t.c0, 8 * kSplitN, &sm.efull[es]);
           const int ksteps = pr.ksteps;
-          const signed char* asrc = g.As + pr.a_off + (long long)(t.r0 / kSplitM) * ksteps * a_bytes;
-          const signed char* bsrc = g.Bs + pr.b_off + (long long)(t.c0 / kSplitN) * ksteps * b_bytes;
+          const signed char* asrc = a.As + pr.a_off + (long long)(t.r0 / kSplitM) * ksteps * a_bytes;
+          const signed char* bsrc = a.Bs + pr.b_off + (long long)(t.c0 / kSplitN) * ksteps * b_bytes;
           for (int ks = 0; ks < ksteps; ++ks, ++n) {
             const int st = (int)(n % kSplitStages);
             const unsigned ph = (unsigned)((n / kSplitStages) & 1);
@@ -603,10 +626,13 @@ __global__ void __maxnreg__(112) k_split(SplitArgs g) {
       long long n = 0, q = 0;
       bool ok = true;
       for (int item = blockIdx.x; ok && item < g.nwork; item += gridDim.x) {
-        const SplitItem t = g.items[item];
-        const int pe = g.alpha_zero ? t.pb : t.pe;
+        int li;
+        const SplitArgs& a = split_req(g, item, li);
+        if (a.flags[kFlagNonFinite]) continue;
+        const SplitItem t = a.items[li];
+        const int pe = a.alpha_zero ? t.pb : t.pe;
         for (int p = t.pb; ok && p < pe; ++p, ++q) {
-          const int ksteps = g.prs[p].ksteps;
+          const int ksteps = a.prs[p].ksteps;
           const int buf = (int)(q & 1);
           if (!split_wait(&sm.tempty[buf], (unsigned)(((q >> 1) & 1) ^ 1), abort, g)) { ok = false; break; }
           tc_fence_after();
@@ -643,9 +669,15 @@ __global__ void __maxnreg__(112) k_split(SplitArgs g) {
     const unsigned tlane = (unsigned)(quarter * 32) << 16;
     long long q = 0, ni = 0;
     bool ok = true;
-    for (int item = blockIdx.x; ok && item < g.nwork; item += gridDim.x, ++ni) {
+    for (int item = blockIdx.x; ok && item < g.nwork; item += gridDim.x) {
+      int li;
+      const SplitArgs& a = split_req(g, item, li);
+      if (a.flags[kFlagNonFinite]) continue;
+      // some row or column exponent of this request lies outside the scale-folded range
+      const bool general = a.flags[kFlagGeneralExp] != 0;
       const int is = (int)(ni % kTileSlots);
       if (!split_wait(&sm.ifull[is], (unsigned)((ni / kTileSlots) & 1), abort, g)) { ok = false; break; }
+      ++ni;
       const SplitTileSlot& ts = sm.tile[is];
       const SplitItem t = ts.rec;
       const bool row_in = row < t.mt;
@@ -660,14 +692,14 @@ __global__ void __maxnreg__(112) k_split(SplitArgs g) {
       fence_proxy_async_smem();
       __syncwarp();
       if (lane == 0) mbar_arrive(&sm.iempty[is]);
-      double* cptr = g.C + t.cbase;
+      double* cptr = a.C + t.cbase;
       double acc[8];
 #pragma unroll
       for (int j = 0; j < 8; ++j) {
         const bool in = row_in && cq * 8 + j < t.nt;
-        acc[j] = (g.beta_zero || !in) ? 0.0 : __dmul_rn(g.beta, cptr[roff + coff[j]]);
+        acc[j] = (a.beta_zero || !in) ? 0.0 : __dmul_rn(a.beta, cptr[roff + coff[j]]);
       }
-      const int pe = g.alpha_zero ? t.pb : t.pe;
+      const int pe = a.alpha_zero ? t.pb : t.pe;
       for (int p = t.pb; p < pe; ++p, ++q) {
         const int buf = (int)(q & 1);
         const int es = (int)(q % kExpSlots);
@@ -994,8 +1026,8 @@ void split_slice(sht_plan* p, double alpha, cudaStream_t s) {
   }
 }
 
-void split_launch(sht_plan* p, const SparseArgs& sa, cudaStream_t s) {
-  const int S = p->split_slices;
+// The kernel arguments of one plan's execute (sa: the FP64 view of the same execute).
+static SplitArgs split_args(sht_plan* p, const SparseArgs& sa) {
   uint64_t one, bb;
   const double d1 = 1.0;
   std::memcpy(&one, &d1, 8);
@@ -1004,7 +1036,7 @@ void split_launch(sht_plan* p, const SparseArgs& sa, cudaStream_t s) {
   g.beta = sa.sc.beta;
   g.beta_zero = sa.sc.beta_zero;
   g.alpha_zero = sa.sc.alpha_zero;
-  g.S = S;
+  g.S = p->split_slices;
   g.As = p->sp_a.as<signed char>();
   g.Ae = p->sp_ae.as<short>();
   g.Bs = p->sp_b.as<signed char>();
@@ -1020,13 +1052,60 @@ void split_launch(sht_plan* p, const SparseArgs& sa, cudaStream_t s) {
   g.err = ctx_error_word(p->ctx);
   g.wait_limit = p->ctx->wait_limit > 0 ? p->ctx->wait_limit : (1LL << 22);
   g.drain_limit = 1LL << 26;
+  return g;
+}
+
+void split_launch(sht_plan* p, const SparseArgs& sa, cudaStream_t s) {
+  const SplitArgs g = split_args(p, sa);
   if (g.nwork <= 0) return;
   const int grid = (int)std::min<long long>(split_grid(p->ctx), g.nwork);
-  kSplitKernels[split_narrow(p, S) ? 1 : 0][S - 1]<<<grid, kSplitThreads, kSplitSmemLaunch, s>>>(g);
+  kSplitKernels[split_narrow(p, g.S) ? 1 : 0][g.S - 1]<<<grid, kSplitThreads, kSplitSmemLaunch, s>>>(g);
   SHT_CUDA(cudaGetLastError());
   // an operand held a non-finite value (the slicer's flag): the tensor-core kernel returned at
   // once and the FP64 tiles compute the execute, with IEEE propagation as in the FP64 forms
   fallback_tiles_if(sa, p->d_bwork.as<int4>(), g.nwork, p->sp_err + kFlagNonFinite, p->ctx->num_sms * 4, s);
+}
+
+int split_kind(const sht_plan* p) { return p->split_slices * 2 + (split_narrow(p, p->split_slices) ? 1 : 0); }
+
+size_t split_desc_bytes() { return sizeof(SplitArgs) + sizeof(int); }
+
+bool split_flags_clear(sht_plan* p, cudaStream_t s) {
+  int f[2] = {0, 0};
+  SHT_CUDA(cudaMemcpyAsync(f, p->sp_err, 8, cudaMemcpyDeviceToHost, s));
+  SHT_CUDA(cudaStreamSynchronize(s));
+  return f[kFlagNonFinite] == 0 && f[kFlagGeneralExp] == 0;
+}
+
+long long split_multi_launch(sht_ctx* ctx, const std::vector<sht_plan*>& plans, const std::vector<SparseArgs>& args,
+                             void* host_descs, PoolBuf& descs, cudaStream_t s) {
+  if (plans.empty()) return 0;
+  const int kind = split_kind(plans[0]);
+  const size_t n = plans.size();
+  SplitArgs* h = static_cast<SplitArgs*>(host_descs);
+  int* first = reinterpret_cast<int*>(h + n);
+  long long total = 0;
+  for (size_t i = 0; i < n; ++i) {
+    if (split_kind(plans[i]) != kind) fail(SHT_ERR_STATE, "one split launch needs one slice count and reassembly");
+    h[i] = split_args(plans[i], args[i]);
+    first[i] = (int)total;
+    total += h[i].nwork;
+    if (total > (long long)INT32_MAX) fail(SHT_ERR_UNSUPPORTED, "split launch above 2^31 tiles");
+  }
+  if (total == 0) return 0;
+  const size_t bytes = n * sizeof(SplitArgs) + n * sizeof(int);
+  descs = PoolBuf(ctx->pool.get(), bytes, s);
+  SHT_CUDA(cudaMemcpyAsync(descs.ptr, h, bytes, cudaMemcpyHostToDevice, s));
+  SplitArgs g = h[0];
+  g.nwork = (int)total;
+  g.multi = descs.as<SplitArgs>();
+  g.mfirst = reinterpret_cast<const int*>(descs.as<SplitArgs>() + n);
+  g.nmulti = (int)n;
+  const int S = plans[0]->split_slices;
+  const int grid = (int)std::min<long long>(split_grid(ctx), total);
+  kSplitKernels[kind & 1][S - 1]<<<grid, kSplitThreads, kSplitSmemLaunch, s>>>(g);
+  SHT_CUDA(cudaGetLastError());
+  return total;
 }
 
 // ------------------------------------------------------------------ INT8 tensor-core peak

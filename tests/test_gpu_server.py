@@ -72,6 +72,31 @@ def test_mix_equals_alone(ctx):
     assert sum(r["flops"] for r in reps) > 0
 
 
+def test_split_mix_equals_split_alone(ctx):
+    # a split-form server: every result bit-identical to sht_contract in split mode alone; a
+    # request whose operand holds a NaN is served in the batched FP64 form (its report says so)
+    # and equals the FP64 forms alone
+    ws = small_mix(17, 8)
+    bad = W.c0(seed=5, nblocks=5, p=0.5)
+    bad.A.data[7] = np.nan
+    ws.append(bad)
+    with sht.Server(ctx, mode=sht.Mode.SPLIT) as srv:
+        held = [(dev(ctx, w.A), dev(ctx, w.B), dev(ctx, w.C)) for w in ws]
+        rids = [srv.submit(w.expr, 1.0, A, B, 0.0, C, w.screen_eps) for w, (A, B, C) in zip(ws, held)]
+        reps = [srv.wait(r, 60) for r in rids]
+        st = srv.stats()
+    assert st["completed"] == len(ws) and st["failed"] == 0
+    assert [r["form"] for r in reps[:-1]] == [int(sht.Mode.SPLIT)] * (len(ws) - 1)
+    assert reps[-1]["form"] == int(sht.Mode.BATCHED_FP64)
+    assert max(r["batch_size"] for r in reps[:-1]) > 1, "split requests submitted together should share a launch"
+    for w, (A, B, C), rep in zip(ws, held, reps):
+        got_ids, got_offs, _ = C.get_sparse_info()
+        got = C.download()
+        ids, offs, data = alone(ctx, w, sht.Mode.SPLIT if rep["form"] == int(sht.Mode.SPLIT) else sht.Mode.PLAIN_FP64)
+        assert np.array_equal(got_ids, ids) and np.array_equal(got_offs, offs), w.name
+        assert bits_equal(got, data), w.name
+
+
 def test_alpha_beta_and_existing_c(ctx):
     rng = np.random.default_rng(3)
     ws = [W.c1(seed=21, scale=0.12, occupancy=0.2), W.c0(seed=4, nblocks=8, p=0.3)]
