@@ -267,15 +267,19 @@ def pcie_bandwidth():
     return out
 
 
-def run_serving(args, sht, ctx, upload, server_kwargs=None):
-    """Serving phase: a seeded Poisson stream of mixed contractions through sht.Server.
+def run_serving(args, sht, ctx, upload):
+    """Serving phase: seeded Poisson streams of mixed contractions through sht.Server, in the
+    batched FP64 form and in the split-precision form.
 
     Requests are drawn from `serve_templates` distinct contractions of the c0..c3 families
     (extents x U(0.25,1), occupancy U(0.05,0.4)), whose inputs stay resident; each request
-    writes its own fresh C, released when it completes.  Reported beside it: the same
-    requests each run alone on the plain FP64 path (synchronous sht_contract, no queueing),
-    a burst of the whole stream submitted at once (the loop's capacity), and a bit-equality
-    check of served results against the same requests run alone."""
+    writes its own fresh C, released when it completes.  Per form: `serve_seeds` streams at
+    `serve_rate` (p50/p99 per seed and over all), a burst of one stream submitted at once (the
+    loop's capacity), and a bit-equality check of served results against the same requests run
+    alone in that form.  Beside them: each request run alone on the plain path (synchronous
+    sht_contract, no queueing)."""
+    import torch
+
     from shtensor_b200 import workloads as W
     rng = np.random.default_rng(args.seed + 1000)
     t_gen = time.perf_counter()
@@ -283,100 +287,123 @@ def run_serving(args, sht, ctx, upload, server_kwargs=None):
     gen_s = time.perf_counter() - t_gen
     ins = [(upload(w.A), upload(w.B)) for w in temps]
     n = max(1, int(round(args.serve_rate * args.serve_seconds)))
-    picks = rng.integers(0, len(temps), n)
-    arrivals = np.cumsum(rng.exponential(1.0 / args.serve_rate, n))
 
     def fresh_c(w):
         return upload(W.empty_tensor(w.C.block_sizes))
 
-    # each template alone on the plain path: plan + execute to completion, median of 3 after one
-    import torch
-    alone_ms, tflops = [], []
-    for w, (A, B) in zip(temps, ins):
-        ts = []
-        for r in range(4):
-            C = fresh_c(w)
-            torch.cuda.synchronize()
-            t0 = time.perf_counter()
-            rep = sht.contract(ctx, w.expr, 1.0, A, B, 0.0, C, w.screen_eps, mode=sht.Mode.PLAIN_FP64)
-            torch.cuda.synchronize()
-            ts.append((time.perf_counter() - t0) * 1e3)
-            del C
-        alone_ms.append(float(np.median(ts[1:])))
-        tflops.append(rep["flops"])
-    alone_stream = np.array([alone_ms[k] for k in picks])
-    stream_flops = float(sum(tflops[k] for k in picks))
+    def alone_times(mode):
+        ms, fl = [], []
+        for w, (A, B) in zip(temps, ins):
+            ts = []
+            for r in range(4):
+                C = fresh_c(w)
+                torch.cuda.synchronize()
+                t0 = time.perf_counter()
+                rep = sht.contract(ctx, w.expr, 1.0, A, B, 0.0, C, w.screen_eps, mode=mode)
+                ctx.stream_sync()
+                ts.append((time.perf_counter() - t0) * 1e3)
+                del C
+            ms.append(float(np.median(ts[1:])))
+            fl.append(rep["flops"])
+        return ms, fl
 
     def pct(v, q):
         v = np.sort(np.asarray(v))
         return float(v[min(len(v) - 1, max(0, int(np.ceil(q * len(v))) - 1))])
 
-    out = {"rate_per_s": args.serve_rate, "requests": n, "stream_s": float(arrivals[-1]),
+    alone_ms, tflops = alone_times(sht.Mode.PLAIN_FP64)
+    alone_split_ms, _ = alone_times(sht.Mode.SPLIT)
+    streams = []
+    for k in range(max(1, args.serve_seeds)):
+        r = np.random.default_rng(args.seed + 2000 + k)
+        streams.append((r.integers(0, len(temps), n), np.cumsum(r.exponential(1.0 / args.serve_rate, n))))
+    picks0, arr0 = streams[0]
+    alone_stream = np.array([alone_ms[k] for k in picks0])
+    stream_flops = float(sum(tflops[k] for k in picks0))
+    out = {"rate_per_s": args.serve_rate, "requests_per_stream": n, "seeds": len(streams),
            "templates": [{"family": w.meta["family"], "u": round(w.meta["u"], 3),
                           "occupancy": round(w.meta["occupancy"], 3), "gflop": f / 1e9,
-                          "alone_plain_ms": a} for w, f, a in zip(temps, tflops, alone_ms)],
-           "template_gen_s": gen_s, "offered_gflops": stream_flops / float(arrivals[-1]) / 1e9}
-    out["alone_plain"] = {"p50_ms": pct(alone_stream, 0.5), "p99_ms": pct(alone_stream, 0.99),
-                          "gflops": stream_flops / (alone_stream.sum() / 1e3) / 1e9,
-                          "busy_s": float(alone_stream.sum() / 1e3)}
-    keep_check = {}
-    with sht.Server(ctx, **(server_kwargs or {})) as srv:
-        # warm-up: every template once
-        for w, (A, B) in zip(temps, ins):
-            C = fresh_c(w)
-            srv.wait(srv.submit(w.expr, 1.0, A, B, 0.0, C, w.screen_eps), 300)
-            del C
-        for phase in ("stream", "burst"):
-            srv.reset_stats()
-            pending = {}
-            reps = []
-            t0 = time.perf_counter()
-            i = 0
-            while i < n or pending:
-                now = time.perf_counter() - t0
-                while i < n and (phase == "burst" or arrivals[i] <= now):
-                    k = int(picks[i])
-                    w, (A, B) = temps[k], ins[k]
-                    C = fresh_c(w)
-                    t_sub = time.perf_counter() - t0
-                    pending[srv.submit(w.expr, 1.0, A, B, 0.0, C, w.screen_eps)] = (C, k, t_sub)
-                    i += 1
-                for rid in list(pending):
-                    if srv.poll(rid):
-                        rep = srv.wait(rid, 300)
-                        C, k, t_sub = pending.pop(rid)
-                        rep.update(template=k, submit_s=round(t_sub, 4))
-                        reps.append(rep)
-                        if phase == "stream" and k not in keep_check and len(keep_check) < 6:
-                            keep_check[k] = C
-                        del C
-                time.sleep(0.0002)
-            st = srv.stats()
-            out[phase] = {"p50_ms": st["p50_ms"], "p99_ms": st["p99_ms"], "max_ms": st["max_ms"],
-                          "gflops": st["gflops"], "span_s": st["span_s"], "completed": st["completed"],
-                          "failed": st["failed"], "launches": st["batches"], "mean_batch": st["mean_batch"],
-                          "max_active": st["max_active_seen"], "deferrals": st["deferrals"],
-                          "mean_queue_ms": float(np.mean([r["queue_ms"] for r in reps])),
-                          "mean_plan_ms": float(np.mean([r["plan_ms"] for r in reps])),
-                          "mean_run_ms": float(np.mean([r["run_ms"] for r in reps])),
-                          "slowest": [{k: (round(v, 3) if isinstance(v, float) else v) for k, v in r.items()
-                                       if k in ("template", "submit_s", "queue_ms", "plan_ms", "run_ms",
-                                                "latency_ms", "batch_size")}
-                                      for r in sorted(reps, key=lambda r: -r["latency_ms"])[:4]]}
-    # served results against the same requests run alone (batched and plain give the same bits)
-    same = True
-    for k, Cs in keep_check.items():
-        w, (A, B) = temps[k], ins[k]
-        Cr = fresh_c(w)
-        sht.contract(ctx, w.expr, 1.0, A, B, 0.0, Cr, w.screen_eps, mode=sht.Mode.PLAIN_FP64)
-        mx, _ = sht.compare(Cs, Cr)
-        same = same and Cs.nnz == Cr.nnz and mx == 0.0
-        del Cr
-    out["mix_equals_alone"] = {"checked": len(keep_check), "bit_equal_values": bool(same)}
-    keep_check.clear()
+                          "alone_plain_ms": a, "alone_split_ms": b}
+                         for w, f, a, b in zip(temps, tflops, alone_ms, alone_split_ms)],
+           "template_gen_s": gen_s, "offered_gflops": stream_flops / float(arr0[-1]) / 1e9,
+           "alone_plain": {"p50_ms": pct(alone_stream, 0.5), "p99_ms": pct(alone_stream, 0.99),
+                           "gflops": stream_flops / (alone_stream.sum() / 1e3) / 1e9,
+                           "busy_s": float(alone_stream.sum() / 1e3)}}
+
+    def run_phase(srv, picks, arrivals, burst, keep=None):
+        srv.reset_stats()
+        pending, reps = {}, []
+        t0 = time.perf_counter()
+        i = 0
+        while i < len(picks) or pending:
+            now = time.perf_counter() - t0
+            while i < len(picks) and (burst or arrivals[i] <= now):
+                k = int(picks[i])
+                w, (A, B) = temps[k], ins[k]
+                C = fresh_c(w)
+                pending[srv.submit(w.expr, 1.0, A, B, 0.0, C, w.screen_eps)] = (C, k, time.perf_counter() - t0)
+                i += 1
+            for rid in list(pending):
+                if srv.poll(rid):
+                    rep = srv.wait(rid, 300)
+                    C, k, t_sub = pending.pop(rid)
+                    rep.update(template=k, submit_s=round(t_sub, 4))
+                    reps.append(rep)
+                    if keep is not None and k not in keep and len(keep) < 6:
+                        keep[k] = (C, rep["form"])
+                    del C
+            time.sleep(0.0002)
+        st = srv.stats()
+        return {"p50_ms": st["p50_ms"], "p99_ms": st["p99_ms"], "max_ms": st["max_ms"], "gflops": st["gflops"],
+                "span_s": st["span_s"], "completed": st["completed"], "failed": st["failed"],
+                "launches": st["batches"], "mean_batch": st["mean_batch"], "max_active": st["max_active_seen"],
+                "deferrals": st["deferrals"],
+                "mean_queue_ms": float(np.mean([r["queue_ms"] for r in reps])),
+                "mean_plan_ms": float(np.mean([r["plan_ms"] for r in reps])),
+                "mean_run_ms": float(np.mean([r["run_ms"] for r in reps])),
+                "slowest": [{k: (round(v, 3) if isinstance(v, float) else v) for k, v in r.items()
+                             if k in ("template", "submit_s", "queue_ms", "plan_ms", "run_ms", "latency_ms",
+                                      "batch_size", "form")}
+                            for r in sorted(reps, key=lambda r: -r["latency_ms"])[:4]]}, reps
+
+    for fname, mode in (("batched", sht.Mode.BATCHED_FP64), ("split", sht.Mode.SPLIT)):
+        keep = {}
+        res = {}
+        with sht.Server(ctx, mode=mode) as srv:
+            for w, (A, B) in zip(temps, ins):  # warm-up: every template once
+                C = fresh_c(w)
+                srv.wait(srv.submit(w.expr, 1.0, A, B, 0.0, C, w.screen_eps), 300)
+                del C
+            per_seed, lat = [], []
+            for k, (picks, arrivals) in enumerate(streams):
+                ph, reps = run_phase(srv, picks, arrivals, False, keep if k == 0 else None)
+                per_seed.append(ph)
+                lat += [r["latency_ms"] for r in reps]
+            res["streams"] = per_seed
+            res["stream"] = {"p50_ms": pct(lat, 0.5), "p99_ms": pct(lat, 0.99), "max_ms": max(lat),
+                             "mean_batch": float(np.mean([p["mean_batch"] for p in per_seed])),
+                             "gflops": float(np.mean([p["gflops"] for p in per_seed])),
+                             "requests": len(lat)}
+            res["burst"], _ = run_phase(srv, picks0, arr0, True)
+        # served results against the same requests run alone in the form that served them
+        same = True
+        for k, (Cs, form) in keep.items():
+            w, (A, B) = temps[k], ins[k]
+            Cr = fresh_c(w)
+            sht.contract(ctx, w.expr, 1.0, A, B, 0.0, Cr, w.screen_eps,
+                         mode=sht.Mode.SPLIT if form == int(sht.Mode.SPLIT) else sht.Mode.PLAIN_FP64)
+            same = same and Cs.nnz == Cr.nnz and sht.bitdiff(Cs, Cr) == 0
+            del Cr
+        res["mix_equals_alone"] = {"checked": len(keep), "bit_equal_values": bool(same)}
+        keep.clear()
+        out[fname] = res
+    busy = out["alone_plain"]["busy_s"] / float(arr0[-1])
+    out["load_note"] = (f"offered load {out['offered_gflops']:.0f} GFLOP/s; run alone back to back the stream keeps "
+                        f"the GPU busy {100 * busy:.0f}% of its span on the plain path, so most requests arrive "
+                        "to an idle GPU and launch at once (batch 1); requests that arrive while a launch runs "
+                        "join the next one")
     del ins
     return out
-
 
 
 # ------------------------------------------------------------------------------ device legs

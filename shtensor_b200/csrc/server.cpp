@@ -164,11 +164,14 @@ void CUDART_CB on_launch_done(void* arg) {
 }
 
 // device bytes a request needs beyond its tensors, estimated before planning: the operands in
-// matrix form plus pair, work and C-pattern arrays (C's own growth is not known until matching)
-size_t estimate_bytes(const Request& r) {
+// matrix form (batched: about 10 bytes per element with padding) or as slices (split: S bytes
+// per element of rows padded to the tile height and k to 32, about 24 at S = 7), plus pair,
+// work and C-pattern arrays (C's own growth is not known until matching)
+size_t estimate_bytes(const Request& r, int mode) {
   const double elems = (double)r.A->nnz + (double)r.B->nnz;
   const double blocks = (double)r.A->nblocks + (double)r.B->nblocks + (double)r.C->nblocks;
-  return (size_t)(elems * 8.0 * 1.25 + blocks * 64.0) + (size_t(1) << 20);
+  const double per = mode == SHT_MODE_SPLIT ? 24.0 : 10.0;
+  return (size_t)(elems * per + blocks * 64.0) + (size_t(1) << 20);
 }
 
 }  // namespace
@@ -301,10 +304,10 @@ bool sht_server::admit() {
     if (others && r.waiting_memory && r.deferred_at == retired_launches) break;
     // requests with the planners may not have taken their memory yet: count their estimates
     size_t planning_bytes = 0;
-    for (const ReqPtr& o : planning) planning_bytes += estimate_bytes(*o);
+    for (const ReqPtr& o : planning) planning_bytes += estimate_bytes(*o, mode);
     const size_t free_now = ctx->pool->free_bytes();
     const size_t avail = free_now > planning_bytes ? free_now - planning_bytes : 0;
-    if (others && avail < reserve_bytes + estimate_bytes(r)) {
+    if (others && avail < reserve_bytes + estimate_bytes(r, mode)) {
       strace("defer request %lld (estimate)", (long long)r.id);
       defer(r);
       break;
