@@ -527,7 +527,7 @@ __device__ __forceinline__ void narrow_load(unsigned tb, int (&X)[narrow_nx(S)][
 // is below 2^23 in magnitude (the host checks S * 127^2 * K), so groups combine two by two in
 // 32 bits and each pair converts with one integer operation and one FP64 add.
 template <int S, bool Narrow>
-__global__ void __maxnreg__(112) k_split(const __grid_constant__ SplitArgs g) {
+__global__ void __launch_bounds__(kSplitThreads, 1) k_split(const __grid_constant__ SplitArgs g) {
   // an operand holds a non-finite value: the FP64 tile kernel computes this execute (in a
   // launch of several requests every role skips such a request's tiles alike)
   if (g.nmulti == 0 && g.flags[kFlagNonFinite]) return;
