@@ -179,23 +179,17 @@ def pair_flops_per_a_block(w) -> np.ndarray:
 
 
 def sample_workload(w, target_flops: float):
-    """The same contraction with A restricted to its blocks of mode-0 index below k, k chosen
-    so that the sample's pair flops reach about target (a bounded CPU sample)."""
+    """The same contraction with A restricted to its first stored blocks, as many as make the
+    sample's pair flops reach about target (a bounded CPU sample)."""
     from shtensor_b200 import workloads as W
-    idx0 = w.A.index_lists()[0]
-    fl = pair_flops_per_a_block(w)
-    n0 = len(w.A.block_sizes[0])
-    per0 = np.zeros(n0)
-    np.add.at(per0, idx0, fl)
-    k = 1
-    while k < n0 and per0[:k].sum() < target_flops:
-        k += 1
-    keep = idx0 < k
-    sizes = w.A.block_dims().prod(axis=1)
-    offs = np.concatenate([[0], np.cumsum(sizes[keep])[:-1]]).astype(np.int64)
-    data = np.concatenate([w.A.data[o:o + s] for o, s in zip(w.A.offsets[keep], sizes[keep])])
-    A = W.HostBlockSparse(w.A.block_sizes, w.A.ids[keep], offs, data)
-    return W.Workload(w.name, w.expr, A, w.B, w.C, screen_eps=w.screen_eps), k, n0
+    fl = np.cumsum(pair_flops_per_a_block(w))
+    n = len(w.A.ids)
+    k = int(min(n, max(1, np.searchsorted(fl, target_flops) + 1)))
+    sizes = w.A.block_dims().prod(axis=1)[:k]
+    offs = np.concatenate([[0], np.cumsum(sizes)[:-1]]).astype(np.int64)
+    data = w.A.data[:int(w.A.offsets[k - 1] + sizes[-1])].copy()
+    A = W.HostBlockSparse(w.A.block_sizes, w.A.ids[:k], offs, data)
+    return W.Workload(w.name, w.expr, A, w.B, w.C, screen_eps=w.screen_eps), k, n
 
 
 def cpu_leg(w, seconds: float, nthreads: int, ref: bool, runs: int):
@@ -220,7 +214,7 @@ def cpu_leg(w, seconds: float, nthreads: int, ref: bool, runs: int):
             else "the oracle's XMM-order restatement (bit-exact to the asmjit kernel's order)")
     return {"value": float(np.median(vals)), "unit": "GFLOP/s", "cores": nthreads, "runs": len(vals),
             "seconds_median": float(np.median(secs)), "kind": "reference" if ref else "port",
-            "sample": (f"A restricted to mode-0 blocks 0..{k - 1} of {n0}: {npairs} pairs, {flops / 1e9:.3f} GFLOP; "
+            "sample": (f"A restricted to its first {k} of {n0} stored blocks: {npairs} pairs, {flops / 1e9:.3f} GFLOP; "
                        f"{what}; OpenMP over C blocks, {nthreads} thread(s)")}
 
 
@@ -522,12 +516,17 @@ def roofline_of(fname, flops, kern_ms, peaks, S=7):
 
 
 def workload_leg(sht, ctx, w, forms, steps, warmup, stream, T, barrier, max_over_ranks, world, peaks,
-                 check=True, tol=1e-12, sweep=(), autotune=False):
+                 check=True, tol=1e-12, sweep=(), autotune=False, clocks=None):
     """Time every form on one workload (full contraction and execute-only), check each against
-    the oracle and give its roofline."""
+    the oracle and give its roofline.  clocks: a dict that receives the clock samples taken
+    while the forms were timed."""
+    import torch
     A, B, C = T(w.A), T(w.B), T(w.C)
     res = {}
     flops = None
+    cs = ClockSampler(torch.cuda.current_device()) if clocks is not None else None
+    if cs:
+        cs.__enter__()
     for fname in forms:
         mode = form_mode(sht, fname)
         if fname == "batched" and autotune:
@@ -542,6 +541,9 @@ def workload_leg(sht, ctx, w, forms, steps, warmup, stream, T, barrier, max_over
              "exec_gflops": flops / ex["exec_ms"] / 1e6, "kernel": FORM_KERNEL[fname]}
         r["roofline"] = roofline_of(fname, prep["flops"], ex["exec_ms"], peaks, prep.get("slices") or 7)
         res[fname] = r
+    if cs:
+        cs.__exit__(None, None, None)
+        clocks.update(cs.summary())
     sweep_out, oinfo = {}, None
     if check:
         par, sweep_out, oinfo = oracle_parity(sht, ctx, w, A, B, list(res), T, stream, sweep)
@@ -595,7 +597,8 @@ def run_ours(args):
         torch.cuda.set_device(0)
     dev = torch.cuda.current_device()
     ctx = sht.Context(int(args.pool_gb * (1 << 30)), device=dev)
-    stream = torch.cuda.current_stream()
+    # a stream of the benchmark's own: graph replay needs a non-default stream
+    stream = torch.cuda.Stream()
 
     def T(h):
         t = sht.Tensor(ctx, h.block_sizes)
@@ -613,12 +616,11 @@ def run_ours(args):
     w = build_workload(args.workload, args.seed, args.scale)
     check = not args.no_oracle and world == 1 and rank == 0
 
-    # ---- headline workload: every form timed, checked against the oracle, clocks sampled
-    with ClockSampler(dev) as cs:
-        results, flops, sweep, oinfo = workload_leg(
-            sht, ctx, w, forms, args.steps, args.warmup, stream, T, barrier, reduce_max, world, peaks, check=check,
-            tol=args.split_tol, sweep=(5, 6) if "split" in forms else (), autotune=not args.no_autotune)
-    clocks = cs.summary()
+    # ---- headline workload: every form timed (clocks sampled meanwhile), checked against the oracle
+    clocks = {}
+    results, flops, sweep, oinfo = workload_leg(
+        sht, ctx, w, forms, args.steps, args.warmup, stream, T, barrier, reduce_max, world, peaks, check=check,
+        tol=args.split_tol, sweep=(5, 6) if "split" in forms else (), autotune=not args.no_autotune, clocks=clocks)
     eligible = [k for k in results if results[k].get("fp64_accurate", True)]
     best = max(eligible, key=lambda k: results[k]["gflops"])
     if "split" in results:
