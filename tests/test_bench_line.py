@@ -41,3 +41,21 @@ def test_reference_arm_other_ranks_stay_silent():
     out = run_bench("--impl", "reference", "--steps", "1", "--warmup", "1", "--scale", "0.25",
                     "--cpu-sample-seconds", "2", env={"RANK": "1", "WORLD_SIZE": "2", "LOCAL_RANK": "1"})
     assert not [l for l in out.strip().splitlines() if l.startswith("{")], out
+
+
+def test_cpu_sample_flop_accounting_matches_the_oracle():
+    # the per-A-block pair flops that size the CPU samples add up to the oracle's flop count,
+    # on the whole workload and on a sample of its first stored A blocks
+    import numpy as np
+
+    import bench
+    import oracle
+    from shtensor_b200 import workloads as W
+    w = W.c1(seed=3, scale=0.25, occupancy=0.4)
+    fl = bench.pair_flops_per_a_block(w)
+    r = oracle.contract(w.expr, 1.0, bench.host(w.A), bench.host(w.B), 0.0, bench.host(w.C))
+    assert np.isclose(fl.sum(), r.flops, rtol=1e-12)
+    samp, k, n = bench.sample_workload(w, 0.3 * r.flops)
+    assert 0 < k < n
+    rs = oracle.contract(samp.expr, 1.0, bench.host(samp.A), bench.host(samp.B), 0.0, bench.host(samp.C))
+    assert np.isclose(fl[:k].sum(), rs.flops, rtol=1e-12) and rs.flops >= 0.3 * r.flops
