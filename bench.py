@@ -356,8 +356,8 @@ def run_serving(args, sht, ctx, upload):
                 "mean_plan_ms": float(np.mean([r["plan_ms"] for r in reps])),
                 "mean_run_ms": float(np.mean([r["run_ms"] for r in reps])),
                 "slowest": [{k: (round(v, 3) if isinstance(v, float) else v) for k, v in r.items()
-                             if k in ("template", "submit_s", "queue_ms", "plan_ms", "run_ms", "latency_ms",
-                                      "batch_size", "form")}
+                             if k in ("template", "submit_s", "queue_ms", "plan_ms", "run_ms", "gpu_ms",
+                                      "latency_ms", "batch_size", "form")}
                             for r in sorted(reps, key=lambda r: -r["latency_ms"])[:4]]}, reps
 
     for fname, mode in (("batched", sht.Mode.BATCHED_FP64), ("split", sht.Mode.SPLIT)):

@@ -236,6 +236,7 @@ typedef struct {
   double queue_ms;       /* submit -> planning starts */
   double plan_ms;        /* planning (matching, C pattern, work list, matrix-form layout) */
   double run_ms;         /* launch -> completion observed */
+  double gpu_ms;         /* device time of its launch: the exec stream reaching it -> done */
   double latency_ms;     /* submit -> completion observed */
   int64_t batch;         /* id of the launch that computed it (-1 if it never ran) */
   int form;              /* the form that computed it (an sht_mode value) */

@@ -78,7 +78,7 @@ class ServerConfig(C.Structure):
 
 class RequestReport(C.Structure):
     _fields_ = [("status", C.c_int), ("npairs", C.c_int64), ("flops", C.c_double), ("queue_ms", C.c_double),
-                ("plan_ms", C.c_double), ("run_ms", C.c_double), ("latency_ms", C.c_double),
+                ("plan_ms", C.c_double), ("run_ms", C.c_double), ("gpu_ms", C.c_double), ("latency_ms", C.c_double),
                 ("batch", C.c_int64), ("form", C.c_int), ("batch_size", C.c_int), ("deferrals", C.c_int)]
 
     def as_dict(self):

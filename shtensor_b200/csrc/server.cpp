@@ -55,6 +55,7 @@ struct Request {
   sht_norm norm = SHT_NORM_FROBENIUS;
   sht_tensor *A = nullptr, *B = nullptr, *C = nullptr;
   Clock::time_point t_submit, t_plan0, t_plan1, t_launch, t_done;
+  double gpu_ms = 0.0;  // device time of its launch (exec stream reaching it -> done)
   std::unique_ptr<sht_plan> plan;
   cudaStream_t pstream = nullptr;  // the planner stream that planned it
   cudaEvent_t planned = nullptr;   // recorded on pstream after its planning work
@@ -80,7 +81,7 @@ struct Launch {
   int slot = 0;
   std::vector<ReqPtr> reqs;
   sht::PoolBuf descs, counter;
-  cudaEvent_t done = nullptr;
+  cudaEvent_t start = nullptr, done = nullptr;  // timed: the launch's device duration
 };
 
 bool touches(const Request& r, const sht_tensor* t) { return r.A == t || r.B == t || r.C == t; }
@@ -225,12 +226,19 @@ bool sht_server::retire() {
       }
     }
     if (q != cudaSuccess) (void)cudaGetLastError();
+    float gms = 0.0f;
+    if (q == cudaSuccess && cudaEventElapsedTime(&gms, l.start, l.done) != cudaSuccess) (void)cudaGetLastError();
     strace("retire launch %lld (%lld requests)", (long long)l.id, (long long)l.reqs.size());
-    for (const ReqPtr& r : l.reqs) finish(r, st, msg, t);
+    strace("  device time of launch %lld: %lld us", (long long)l.id, (long long)(gms * 1000.0f));
+    for (const ReqPtr& r : l.reqs) {
+      r->gpu_ms = gms;
+      finish(r, st, msg, t);
+    }
     // the launch's work is complete: its buffers may be reused as soon as a planner gets to them
     l.descs.use_on(plan_streams[0]);
     l.counter.use_on(plan_streams[0]);
     slot_busy[l.slot] = false;
+    cudaEventDestroy(l.start);
     cudaEventDestroy(l.done);
     running.pop_front();
     ++retired_launches;
@@ -430,6 +438,8 @@ bool sht_server::launch() {
   const size_t n = l->reqs.size();
   const Clock::time_point t = Clock::now();
   try {
+    SHT_CUDA(cudaEventCreate(&l->start));
+    SHT_CUDA(cudaEventRecord(l->start, exec_stream));
     std::vector<sht_plan*> plans;
     std::vector<sht::SparseArgs> args;
     for (const ReqPtr& r : l->reqs) {
@@ -449,7 +459,7 @@ bool sht_server::launch() {
     }
     l->descs.use_on(exec_stream);
     l->counter.use_on(exec_stream);
-    SHT_CUDA(cudaEventCreateWithFlags(&l->done, cudaEventDisableTiming));
+    SHT_CUDA(cudaEventCreate(&l->done));
     SHT_CUDA(cudaEventRecord(l->done, exec_stream));
     SHT_CUDA(cudaLaunchHostFunc(exec_stream, on_launch_done, this));
     strace("launch %lld with %lld requests", (long long)l->id, (long long)n);
@@ -457,6 +467,7 @@ bool sht_server::launch() {
     // nothing of this launch is known to run: wait for the stream, then fail its requests
     cudaStreamSynchronize(exec_stream);
     (void)cudaGetLastError();
+    if (l->start) cudaEventDestroy(l->start);
     if (l->done) cudaEventDestroy(l->done);
     for (const ReqPtr& r : l->reqs) finish(r, e.code, e.msg, Clock::now());
     return true;
@@ -616,6 +627,7 @@ sht_status sht_server_wait(sht_server* srv, int64_t request_id, double timeout_s
     rep->queue_ms = ms_between(r->t_submit, planned ? r->t_plan0 : r->t_done);
     rep->plan_ms = r->t_plan1 != Clock::time_point{} ? ms_between(r->t_plan0, r->t_plan1) : 0.0;
     rep->run_ms = r->batch >= 0 ? ms_between(r->t_launch, r->t_done) : 0.0;
+    rep->gpu_ms = r->gpu_ms;
     rep->latency_ms = ms_between(r->t_submit, r->t_done);
     rep->batch = r->batch;
     rep->form = r->form;

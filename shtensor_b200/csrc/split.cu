@@ -169,7 +169,11 @@ __global__ void __launch_bounds__(kSliceWarps * 32, 4) k_slice(
       if (pscale) pscale[exp_off[b] + r] = in_range ? ldexp(1.0, e) : 0.0;
     }
     // slices of every chunk of this warp: 16 k at a time, the S slices packed four bytes to a
-    // register and stored as one 16-byte word each
+    // register and stored as one 16-byte word each.  v * 2^-e is exact when 2^-e is a normal
+    // double and the product is normal; a product below 2^-1022 has only zero slices either
+    // way.  Other exponents scale with scalbn.
+    const bool mul = e >= -1022 && e <= 1022;
+    const double inv = mul ? __longlong_as_double((long long)(1023 - e) << 52) : 0.0;
     signed char* o = out + out_off[b] + (long long)(r / R) * ksteps * S * R * kSplitK;
     for (int c = warp; c < nchunks; c += kSliceWarps) {
       double v[16];
@@ -184,12 +188,14 @@ __global__ void __launch_bounds__(kSliceWarps * 32, 4) k_slice(
       for (int t = 0; t < kMaxSlices; ++t) w[t][0] = w[t][1] = w[t][2] = w[t][3] = 0u;
 #pragma unroll
       for (int j = 0; j < 16; ++j) {
-        double x = scalbn(v[j], -e);
+        double x = mul ? v[j] * inv : scalbn(v[j], -e);
 #pragma unroll
         for (int t = 0; t < kMaxSlices; ++t) {
           const double y = x * 128.0;
           const double tr = trunc(y);
-          w[t][j >> 2] |= ((unsigned)(int)tr & 0xffu) << ((j & 3) * 8);
+          // the integer tr (|tr| <= 127) in the low word of 1.5 * 2^52 + tr, exactly
+          const unsigned bits = (unsigned)__double2loint(tr + 6755399441055744.0);
+          w[t][j >> 2] |= (bits & 0xffu) << ((j & 3) * 8);
           x = y - tr;
         }
       }
@@ -452,19 +458,46 @@ struct SplitSmem {
   int abort;
 };
 
-// The request that global item `item` belongs to and its item index there.
-__device__ __forceinline__ const SplitArgs& split_req(const SplitArgs& g, int item, int& li) {
-  if (g.nmulti == 0) {
+// The fields of one request that the roles use, copied into registers once per item: in a
+// launch of one plan they come from the kernel parameters; in a launch of several requests
+// from the request's entry of the device array (read once, not after every memory-clobbering
+// mbarrier or bulk-copy instruction).
+struct SplitReq {
+  const signed char* As; const short* Ae;
+  const signed char* Bs; const short* Be; const double* Bsc;
+  double* C;
+  const int* rowtab; const int* coltab;
+  const SplitItem* items; const SplitPair* prs;
+  double beta;
+  int beta_zero, alpha_zero, flags_nonfinite, flags_general;
+};
+
+__device__ __forceinline__ SplitReq req_fields(const SplitArgs& a, bool read_flags) {
+  SplitReq r;
+  r.As = a.As; r.Ae = a.Ae; r.Bs = a.Bs; r.Be = a.Be; r.Bsc = a.Bsc; r.C = a.C;
+  r.rowtab = a.rowtab; r.coltab = a.coltab; r.items = a.items; r.prs = a.prs;
+  r.beta = a.beta; r.beta_zero = a.beta_zero; r.alpha_zero = a.alpha_zero;
+  r.flags_nonfinite = read_flags ? a.flags[kFlagNonFinite] : 0;
+  r.flags_general = read_flags ? a.flags[kFlagGeneralExp] : 0;
+  return r;
+}
+
+// The request that global item `item` belongs to (Multi: binary search over the requests'
+// first items) and its item index there.
+template <bool Multi>
+__device__ __forceinline__ SplitReq split_req(const SplitArgs& g, int item, int& li) {
+  if constexpr (!Multi) {
     li = item;
-    return g;
+    return req_fields(g, false);
+  } else {
+    int lo = 0, hi = g.nmulti;  // the last request whose first item is <= item
+    while (hi - lo > 1) {
+      const int mid = (lo + hi) >> 1;
+      if (g.mfirst[mid] <= item) lo = mid; else hi = mid;
+    }
+    li = item - g.mfirst[lo];
+    return req_fields(g.multi[lo], true);
   }
-  int lo = 0, hi = g.nmulti;  // the last request whose first item is <= item
-  while (hi - lo > 1) {
-    const int mid = (lo + hi) >> 1;
-    if (g.mfirst[mid] <= item) lo = mid; else hi = mid;
-  }
-  li = item - g.mfirst[lo];
-  return g.multi[lo];
 }
 
 // bounded wait that also gives up when another role raised the abort flag
@@ -526,11 +559,13 @@ __device__ __forceinline__ void narrow_load(unsigned tb, int (&X)[narrow_nx(S)][
 // and of the reassembly unroll completely; one instance per S = 1..8.  Narrow: every group sum
 // is below 2^23 in magnitude (the host checks S * 127^2 * K), so groups combine two by two in
 // 32 bits and each pair converts with one integer operation and one FP64 add.
-template <int S, bool Narrow>
+template <int S, bool Narrow, bool Multi>
 __global__ void __launch_bounds__(kSplitThreads, 1) k_split(const __grid_constant__ SplitArgs g) {
   // an operand holds a non-finite value: the FP64 tile kernel computes this execute (in a
   // launch of several requests every role skips such a request's tiles alike)
-  if (g.nmulti == 0 && g.flags[kFlagNonFinite]) return;
+  if (!Multi && g.flags[kFlagNonFinite]) return;
+  // one plan: some row or column exponent lies outside the scale-folded range (uniform)
+  const bool general1 = !Multi && g.flags[kFlagGeneralExp] != 0;
   extern __shared__ __align__(1024) unsigned char smem_raw[];
   SplitSmem& sm = *reinterpret_cast<SplitSmem*>(smem_raw);
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
@@ -576,8 +611,8 @@ __global__ void __launch_bounds__(kSplitThreads, 1) k_split(const __grid_constan
       bool ok = true;
       for (int item = blockIdx.x; ok && item < g.nwork; item += gridDim.x) {
         int li;
-        const SplitArgs& a = split_req(g, item, li);
-        if (a.flags[kFlagNonFinite]) continue;
+        const SplitReq a = split_req<Multi>(g, item, li);
+        if (a.flags_nonfinite) continue;
         const SplitItem t = a.items[li];
         const int is = (int)(ni % kTileSlots);
         if (!split_wait(&sm.iempty[is], (unsigned)(((ni / kTileSlots) & 1) ^ 1), abort, g)) { ok = false; break; }
@@ -627,8 +662,8 @@ __global__ void __launch_bounds__(kSplitThreads, 1) k_split(const __grid_constan
       bool ok = true;
       for (int item = blockIdx.x; ok && item < g.nwork; item += gridDim.x) {
         int li;
-        const SplitArgs& a = split_req(g, item, li);
-        if (a.flags[kFlagNonFinite]) continue;
+        const SplitReq a = split_req<Multi>(g, item, li);
+        if (a.flags_nonfinite) continue;
         const SplitItem t = a.items[li];
         const int pe = a.alpha_zero ? t.pb : t.pe;
         for (int p = t.pb; ok && p < pe; ++p, ++q) {
@@ -671,10 +706,10 @@ __global__ void __launch_bounds__(kSplitThreads, 1) k_split(const __grid_constan
     bool ok = true;
     for (int item = blockIdx.x; ok && item < g.nwork; item += gridDim.x) {
       int li;
-      const SplitArgs& a = split_req(g, item, li);
-      if (a.flags[kFlagNonFinite]) continue;
+      const SplitReq a = split_req<Multi>(g, item, li);
+      if (a.flags_nonfinite) continue;
       // some row or column exponent of this request lies outside the scale-folded range
-      const bool general = a.flags[kFlagGeneralExp] != 0;
+      const bool general = Multi ? a.flags_general != 0 : general1;
       const int is = (int)(ni % kTileSlots);
       if (!split_wait(&sm.ifull[is], (unsigned)((ni / kTileSlots) & 1), abort, g)) { ok = false; break; }
       ++ni;
@@ -964,11 +999,15 @@ constexpr size_t kSplitSmemLaunch = sizeof(SplitSmem);
 static_assert(kSplitSmemLaunch > 114 * 1024, "one split CTA per SM");
 
 using SplitKernel = void (*)(SplitArgs);
-static const SplitKernel kSplitKernels[2][kMaxSlices] = {
-    {k_split<1, false>, k_split<2, false>, k_split<3, false>, k_split<4, false>, k_split<5, false>,
-     k_split<6, false>, k_split<7, false>, k_split<8, false>},
-    {k_split<1, true>, k_split<2, true>, k_split<3, true>, k_split<4, true>, k_split<5, true>, k_split<6, true>,
-     k_split<7, true>, k_split<8, true>}};
+static const SplitKernel kSplitKernels[2][2][kMaxSlices] = {  // [multi][narrow][S - 1]
+    {{k_split<1, false, false>, k_split<2, false, false>, k_split<3, false, false>, k_split<4, false, false>,
+      k_split<5, false, false>, k_split<6, false, false>, k_split<7, false, false>, k_split<8, false, false>},
+     {k_split<1, true, false>, k_split<2, true, false>, k_split<3, true, false>, k_split<4, true, false>,
+      k_split<5, true, false>, k_split<6, true, false>, k_split<7, true, false>, k_split<8, true, false>}},
+    {{k_split<1, false, true>, k_split<2, false, true>, k_split<3, false, true>, k_split<4, false, true>,
+      k_split<5, false, true>, k_split<6, false, true>, k_split<7, false, true>, k_split<8, false, true>},
+     {k_split<1, true, true>, k_split<2, true, true>, k_split<3, true, true>, k_split<4, true, true>,
+      k_split<5, true, true>, k_split<6, true, true>, k_split<7, true, true>, k_split<8, true, true>}}};
 
 // every group sum below 2^23: S * 127^2 * K for the largest padded contracted extent K (the
 // product of the largest block extents of the contracted modes)
@@ -986,13 +1025,14 @@ static bool split_narrow(const sht_plan* p, int S) {
 static int split_grid(sht_ctx* ctx) {
   static std::once_flag once;
   std::call_once(once, [] {
-    for (const auto& row : kSplitKernels)
-      for (SplitKernel k : row) {
-        SHT_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSplitSmemLaunch));
-        int n = 0;
-        SHT_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k, kSplitThreads, kSplitSmemLaunch));
-        if (n != 1) fail(SHT_ERR_STATE, "split kernel must run one CTA per SM (TMEM budget)");
-      }
+    for (const auto& plane : kSplitKernels)
+      for (const auto& row : plane)
+        for (SplitKernel k : row) {
+          SHT_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSplitSmemLaunch));
+          int n = 0;
+          SHT_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k, kSplitThreads, kSplitSmemLaunch));
+          if (n != 1) fail(SHT_ERR_STATE, "split kernel must run one CTA per SM (TMEM budget)");
+        }
   });
   return ctx->num_sms;
 }
@@ -1059,7 +1099,7 @@ void split_launch(sht_plan* p, const SparseArgs& sa, cudaStream_t s) {
   const SplitArgs g = split_args(p, sa);
   if (g.nwork <= 0) return;
   const int grid = (int)std::min<long long>(split_grid(p->ctx), g.nwork);
-  kSplitKernels[split_narrow(p, g.S) ? 1 : 0][g.S - 1]<<<grid, kSplitThreads, kSplitSmemLaunch, s>>>(g);
+  kSplitKernels[0][split_narrow(p, g.S) ? 1 : 0][g.S - 1]<<<grid, kSplitThreads, kSplitSmemLaunch, s>>>(g);
   SHT_CUDA(cudaGetLastError());
   // an operand held a non-finite value (the slicer's flag): the tensor-core kernel returned at
   // once and the FP64 tiles compute the execute, with IEEE propagation as in the FP64 forms
@@ -1103,7 +1143,7 @@ long long split_multi_launch(sht_ctx* ctx, const std::vector<sht_plan*>& plans, 
   g.nmulti = (int)n;
   const int S = plans[0]->split_slices;
   const int grid = (int)std::min<long long>(split_grid(ctx), total);
-  kSplitKernels[kind & 1][S - 1]<<<grid, kSplitThreads, kSplitSmemLaunch, s>>>(g);
+  kSplitKernels[1][kind & 1][S - 1]<<<grid, kSplitThreads, kSplitSmemLaunch, s>>>(g);
   SHT_CUDA(cudaGetLastError());
   return total;
 }
