@@ -13,7 +13,9 @@
 // previous launch ran join the next one: batching is continuous, not by fixed windows.  The
 // planner streams have the higher priority and a serving launch leaves CTA slots free on
 // every SM, so planning overlaps the running launch; several planners overlap each other's
-// host round trips.  Completion is signalled by a host callback queued after each launch.
+// host round trips.  Completion is signalled by a waiter thread that blocks on an event recorded
+// after each launch (no host function in the exec stream, which would hold back the next launch
+// until the CPU ran it).
 #include <algorithm>
 #include <chrono>
 #include <cmath>
@@ -117,7 +119,7 @@ struct sht_server {
   std::unordered_map<int64_t, ReqPtr> table;
   int64_t next_id = 1;
   bool stop = false, stop_planners = false;
-  int completions = 0;  // completion callbacks not yet handled
+  int completions = 0;  // launch completions seen by the waiter, not yet handled
   // statistics since the last reset
   int64_t submitted = 0, completed = 0, failed = 0, batches = 0, batched_reqs = 0, deferrals = 0;
   int max_active_seen = 0;
@@ -136,6 +138,13 @@ struct sht_server {
   int64_t retired_launches = 0;
   std::thread thread;
   std::vector<std::thread> planner_threads;
+  // completion waiter: blocks on one event per launch and wakes the loop.  A host function
+  // queued on the exec stream would hold back the next launch until the CPU ran it.
+  std::thread waiter_thread;
+  std::deque<cudaEvent_t> wait_q;   // guarded by mu; the waiter destroys each event it took
+  std::condition_variable wait_cv;
+  bool stop_waiter = false;
+  void waiter();
 
   void loop();
   void planner(int index);
@@ -154,15 +163,6 @@ struct sht_server {
 
 namespace {
 
-void CUDART_CB on_launch_done(void* arg) {
-  // runs on a CUDA callback thread: no CUDA calls here
-  sht_server* s = static_cast<sht_server*>(arg);
-  {
-    std::lock_guard<std::mutex> lk(s->mu);
-    ++s->completions;
-  }
-  s->wake.notify_one();
-}
 
 // device bytes a request needs beyond its tensors, estimated before planning: the operands in
 // matrix form (batched: about 10 bytes per element with padding) or as slices (split: S bytes
@@ -461,7 +461,15 @@ bool sht_server::launch() {
     l->counter.use_on(exec_stream);
     SHT_CUDA(cudaEventCreate(&l->done));
     SHT_CUDA(cudaEventRecord(l->done, exec_stream));
-    SHT_CUDA(cudaLaunchHostFunc(exec_stream, on_launch_done, this));
+    // the waiter's own event (blocking sync: the waiter sleeps in the driver, it does not spin)
+    cudaEvent_t w = nullptr;
+    SHT_CUDA(cudaEventCreateWithFlags(&w, cudaEventBlockingSync | cudaEventDisableTiming));
+    SHT_CUDA(cudaEventRecord(w, exec_stream));
+    {
+      std::lock_guard<std::mutex> lk(mu);
+      wait_q.push_back(w);
+    }
+    wait_cv.notify_one();
     strace("launch %lld with %lld requests", (long long)l->id, (long long)n);
   } catch (const sht::Error& e) {
     // nothing of this launch is known to run: wait for the stream, then fail its requests
@@ -482,6 +490,27 @@ bool sht_server::launch() {
   return true;
 }
 
+void sht_server::waiter() {
+  cudaSetDevice(ctx->device);
+  for (;;) {
+    cudaEvent_t ev = nullptr;
+    {
+      std::unique_lock<std::mutex> lk(mu);
+      wait_cv.wait(lk, [&] { return stop_waiter || !wait_q.empty(); });
+      if (wait_q.empty()) return;  // stop_waiter, nothing left to wait for
+      ev = wait_q.front();
+      wait_q.pop_front();
+    }
+    cudaEventSynchronize(ev);  // an error surfaces on the launch's own event in retire()
+    cudaEventDestroy(ev);
+    {
+      std::lock_guard<std::mutex> lk(mu);
+      ++completions;
+    }
+    wake.notify_one();
+  }
+}
+
 void sht_server::loop() {
   cudaSetDevice(ctx->device);
   for (;;) {
@@ -496,7 +525,7 @@ void sht_server::loop() {
       completions = 0;
       continue;
     }
-    // idle: sleep until a submit, a planned request, a completion callback or stop; the
+    // idle: sleep until a submit, a planned request, a completion or stop; the
     // timeout bounds the wait for a launch whose callback cannot arrive (a failed stream)
     if (incoming.empty() && planned.empty())
       wake.wait_for(lk, std::chrono::milliseconds(running.empty() ? 50 : 2),
@@ -552,6 +581,7 @@ sht_status sht_server_create(sht_ctx* ctx, const sht_server_config* cfg, sht_ser
     }
     sht_server* raw = s.get();
     for (int i = 0; i < s->nplanners; ++i) s->planner_threads.emplace_back([raw, i] { raw->planner(i); });
+    s->waiter_thread = std::thread([raw] { raw->waiter(); });
     s->thread = std::thread([raw] { raw->loop(); });
     *out = s.release();
   });
@@ -696,8 +726,14 @@ sht_status sht_server_destroy(sht_server* srv) {
     }
     srv->plan_cv.notify_all();
     for (std::thread& t : srv->planner_threads) t.join();
+    {
+      std::lock_guard<std::mutex> lk(srv->mu);
+      srv->stop_waiter = true;
+    }
+    srv->wait_cv.notify_all();
+    if (srv->waiter_thread.joinable()) srv->waiter_thread.join();  // after its queue is empty
     cudaSetDevice(srv->ctx->device);
-    cudaStreamSynchronize(srv->exec_stream);  // also waits for the last completion callback
+    cudaStreamSynchronize(srv->exec_stream);
     for (cudaStream_t st : srv->plan_streams) {
       cudaStreamSynchronize(st);
       cudaStreamDestroy(st);
