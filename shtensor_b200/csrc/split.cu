@@ -49,7 +49,15 @@
 namespace sht {
 
 constexpr int kSplitM = 128, kSplitN = 32, kSplitK = 32, kMaxSlices = 8;
-constexpr int kSplitStages = 4;
+// Operand stages of the shared-memory ring: as many as fit beside the slots in the 227 KB of
+// one CTA (6 at S = 7).  A stage holds one k-step of one pair, S * 5 KB; the copies of a stage
+// take longer than the tensor core needs for one, so depth hides their latency.
+constexpr int kSplitSmemBudget = 227 * 1024;
+constexpr int kSplitSlotBytes = 8 * 1024;  // tile and exponent rings, barriers (upper bound)
+__host__ __device__ constexpr int split_stages(int S) {
+  return (kSplitSmemBudget - kSplitSlotBytes) / (S * 5 * 1024) > 8 ? 8
+                                                                  : (kSplitSmemBudget - kSplitSlotBytes) / (S * 5 * 1024);
+}
 constexpr int kAChunk = kSplitM * kSplitK;      // bytes of one A slab (128 rows x 32 k)
 constexpr int kBChunk = kSplitN * kSplitK;      // bytes of one B slab (32 columns x 32 k)
 constexpr int kBufCols = kMaxSlices * kSplitN;  // TMEM columns of one accumulator set (8 groups)
@@ -78,15 +86,16 @@ constexpr int kExpLoA = -900, kExpHiA = 960, kExpLoB = -1022, kExpHiB = 1023;
 // One 128-thread CTA per item of 32 rows of one block (items are numbered block after block,
 // istart[b] the first item of block b).  Lane = row; warp w takes the 16-wide k-chunks w, w+4,
 // ... of the row (a warp's load of one k is 32 consecutive rows of a column-major block).  The
-// first chunk of each warp stays in registers (every chunk when K <= 64); the row maximum is
+// chunk of each warp stays in registers when K <= 64 (one chunk per warp); the row maximum is
 // reduced over the four warps in shared memory and gives the row's exponent (rows padded up to
 // the tile height R get 0); then every chunk is cut into its S int8 slices, packed four bytes
 // to a register and stored as one 16-byte word per slice, in tile order:
 //   out[((tile * ksteps + ks) * S + t) * R * 32 + slab_offset(row % R, k)].
 // Rows past the block and k past K are zero.  With pscale set (B columns), the row's scale 2^e
-// is also written as a double (0 when e is outside [elo, ehi]).
+// is also written as a double (0 when e is outside [elo, ehi]).  Rows with more than four
+// chunks (K > 64) read their values a second time for the slicing.
 constexpr int kSliceWarps = 4;
-__global__ void __launch_bounds__(kSliceWarps * 32, 4) k_slice(
+__global__ void __launch_bounds__(kSliceWarps * 32, 5) k_slice(
     const double* __restrict__ src, const long long* __restrict__ src_off, const int* __restrict__ dims, int order,
     ModeMap fm, ModeMap km, const long long* __restrict__ out_off, const long long* __restrict__ exp_off,
     signed char* __restrict__ out, short* __restrict__ expo, double* __restrict__ pscale, int elo, int ehi,
@@ -134,20 +143,13 @@ __global__ void __launch_bounds__(kSliceWarps * 32, 4) k_slice(
         v[j] = (live && k < K) ? __dmul_rn(s[fr + koff(k)], scale) : 0.0;
       }
     };
-    // pass over this warp's chunks: the first stays in registers
-    double v0[16];
+    // pass over this warp's chunks; when the row has at most kSliceWarps chunks (K <= 64) each
+    // warp has at most one, and it stays in registers for the slicing
+    const bool hold = nchunks <= kSliceWarps;
+    double v[16];
     double mx = 0.0;
     bool finite = true;
-    if (warp < nchunks) {
-      load_chunk(warp, v0);
-#pragma unroll
-      for (int j = 0; j < 16; ++j) {
-        finite = finite && isfinite(v0[j]);
-        mx = fmax(mx, fabs(v0[j]));
-      }
-    }
-    for (int c = warp + kSliceWarps; c < nchunks; c += kSliceWarps) {
-      double v[16];
+    for (int c = warp; c < nchunks; c += kSliceWarps) {
       load_chunk(c, v);
 #pragma unroll
       for (int j = 0; j < 16; ++j) {
@@ -176,35 +178,25 @@ __global__ void __launch_bounds__(kSliceWarps * 32, 4) k_slice(
     const double inv = mul ? __longlong_as_double((long long)(1023 - e) << 52) : 0.0;
     signed char* o = out + out_off[b] + (long long)(r / R) * ksteps * S * R * kSplitK;
     for (int c = warp; c < nchunks; c += kSliceWarps) {
-      double v[16];
-      if (c == warp) {
+      if (!hold) load_chunk(c, v);
 #pragma unroll
-        for (int j = 0; j < 16; ++j) v[j] = v0[j];
-      } else {
-        load_chunk(c, v);
-      }
-      unsigned w[kMaxSlices][4];
+      for (int j = 0; j < 16; ++j) v[j] = mul ? v[j] * inv : scalbn(v[j], -e);
+      // slice t of the 16 values from their running remainders, stored as soon as it is packed
+      const long long base = (long long)(c / 2) * S * R * kSplitK + slab_offset(r % R, (c & 1) * 16);
+      for (int t = 0; t < S; ++t) {
+        unsigned w[4] = {0u, 0u, 0u, 0u};
 #pragma unroll
-      for (int t = 0; t < kMaxSlices; ++t) w[t][0] = w[t][1] = w[t][2] = w[t][3] = 0u;
-#pragma unroll
-      for (int j = 0; j < 16; ++j) {
-        double x = mul ? v[j] * inv : scalbn(v[j], -e);
-#pragma unroll
-        for (int t = 0; t < kMaxSlices; ++t) {
-          const double y = x * 128.0;
+        for (int j = 0; j < 16; ++j) {
+          const double y = v[j] * 128.0;
           const double tr = trunc(y);
           // the integer tr (|tr| <= 127) in the low word of 1.5 * 2^52 + tr, exactly
           const unsigned bits = (unsigned)__double2loint(tr + 6755399441055744.0);
-          w[t][j >> 2] |= (bits & 0xffu) << ((j & 3) * 8);
-          x = y - tr;
+          w[j >> 2] |= (bits & 0xffu) << ((j & 3) * 8);
+          v[j] = y - tr;
         }
+        *reinterpret_cast<int4*>(o + base + (long long)t * R * kSplitK) =
+            make_int4((int)w[0], (int)w[1], (int)w[2], (int)w[3]);
       }
-      const long long base = (long long)(c / 2) * S * R * kSplitK + slab_offset(r % R, (c & 1) * 16);
-#pragma unroll
-      for (int t = 0; t < kMaxSlices; ++t)
-        if (t < S)
-          *reinterpret_cast<int4*>(o + base + (long long)t * R * kSplitK) =
-              make_int4((int)w[t][0], (int)w[t][1], (int)w[t][2], (int)w[t][3]);
     }
   }
 }
@@ -448,11 +440,13 @@ static_assert(sizeof(SplitItem) % 16 == 0 && kTileSlotBytes == 48 + 4 * (kSplitM
                   kExpSlotBytes == 2 * (kSplitM + kSplitN) + 8 * kSplitN && offsetof(SplitExpSlot, sc) % 16 == 0,
               "slot members are bulk-copy destinations at 16-byte offsets");
 
+template <int S>
 struct SplitSmem {
-  alignas(1024) signed char stage[kSplitStages][kMaxSlices * (kAChunk + kBChunk)];
+  static constexpr int kStages = split_stages(S);
+  alignas(1024) signed char stage[kStages][S * (kAChunk + kBChunk)];
   alignas(16) SplitTileSlot tile[kTileSlots];
   alignas(16) SplitExpSlot ex[kExpSlots];
-  alignas(8) unsigned long long full[kSplitStages], empty[kSplitStages], tfull[2], tempty[2], drain;
+  alignas(8) unsigned long long full[kStages], empty[kStages], tfull[2], tempty[2], drain;
   unsigned long long ifull[kTileSlots], iempty[kTileSlots], efull[kExpSlots], eempty[kExpSlots];
   unsigned tmem_base;
   int abort;
@@ -567,7 +561,9 @@ __global__ void __launch_bounds__(kSplitThreads, 1) k_split(const __grid_constan
   // one plan: some row or column exponent lies outside the scale-folded range (uniform)
   const bool general1 = !Multi && g.flags[kFlagGeneralExp] != 0;
   extern __shared__ __align__(1024) unsigned char smem_raw[];
-  SplitSmem& sm = *reinterpret_cast<SplitSmem*>(smem_raw);
+  using Smem = SplitSmem<S>;
+  constexpr int kSplitStages = Smem::kStages;
+  Smem& sm = *reinterpret_cast<Smem*>(smem_raw);
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   volatile int* abort = &sm.abort;
 
@@ -608,6 +604,8 @@ __global__ void __launch_bounds__(kSplitThreads, 1) k_split(const __grid_constan
     // ---------------------------------------------------------------- producer
     if (lane == 0) {
       long long n = 0, q = 0, ni = 0;
+      int st = 0;         // stage of k-step n (n % kSplitStages) and its ring phase
+      unsigned sph = 0;
       bool ok = true;
       for (int item = blockIdx.x; ok && item < g.nwork; item += gridDim.x) {
         int li;
@@ -622,8 +620,11 @@ __global__ void __launch_bounds__(kSplitThreads, 1) k_split(const __grid_constan
         bulk_g2s(sm.tile[is].rowoff, a.rowtab + t.rtab, 4 * kSplitM, &sm.ifull[is]);
         bulk_g2s(sm.tile[is].coloff, a.coltab + t.ctab, 4 * kSplitN, &sm.ifull[is]);
         const int pe = a.alpha_zero ? t.pb : t.pe;
+        // pair records one ahead: the load of the next is in flight while this pair's copies go out
+        SplitPair pr_next = t.pb < pe ? a.prs[t.pb] : SplitPair{};
         for (int p = t.pb; ok && p < pe; ++p, ++q) {
-          const SplitPair pr = a.prs[p];
+          const SplitPair pr = pr_next;
+          if (p + 1 < pe) pr_next = a.prs[p + 1];
           const int es = (int)(q % kExpSlots);
           if (!split_wait(&sm.eempty[es], (unsigned)(((q / kExpSlots) & 1) ^ 1), abort, g)) { ok = false; break; }
           mbar_expect_tx(&sm.efull[es], kExpSlotBytes);
@@ -634,12 +635,14 @@ __global__ void __launch_bounds__(kSplitThreads, 1) k_split(const __grid_constan
           const signed char* asrc = a.As + pr.a_off + (long long)(t.r0 / kSplitM) * ksteps * a_bytes;
           const signed char* bsrc = a.Bs + pr.b_off + (long long)(t.c0 / kSplitN) * ksteps * b_bytes;
           for (int ks = 0; ks < ksteps; ++ks, ++n) {
-            const int st = (int)(n % kSplitStages);
-            const unsigned ph = (unsigned)((n / kSplitStages) & 1);
-            if (!split_wait(&sm.empty[st], ph ^ 1u, abort, g)) { ok = false; break; }
+            if (!split_wait(&sm.empty[st], sph ^ 1u, abort, g)) { ok = false; break; }
             mbar_expect_tx(&sm.full[st], a_bytes + b_bytes);
             bulk_g2s(sm.stage[st], asrc + (long long)ks * a_bytes, a_bytes, &sm.full[st]);
             bulk_g2s(sm.stage[st] + a_bytes, bsrc + (long long)ks * b_bytes, b_bytes, &sm.full[st]);
+            if (++st == kSplitStages) {
+              st = 0;
+              sph ^= 1u;
+            }
           }
         }
       }
@@ -659,6 +662,8 @@ __global__ void __launch_bounds__(kSplitThreads, 1) k_split(const __grid_constan
     // ---------------------------------------------------------------- MMA issuer
     if (lane == 0) {
       long long n = 0, q = 0;
+      int st = 0;  // stage of k-step n and its ring phase, as the producer's
+      unsigned sph = 0;
       bool ok = true;
       for (int item = blockIdx.x; ok && item < g.nwork; item += gridDim.x) {
         int li;
@@ -666,15 +671,16 @@ __global__ void __launch_bounds__(kSplitThreads, 1) k_split(const __grid_constan
         if (a.flags_nonfinite) continue;
         const SplitItem t = a.items[li];
         const int pe = a.alpha_zero ? t.pb : t.pe;
+        int ks_next = t.pb < pe ? a.prs[t.pb].ksteps : 0;  // one pair ahead, as the producer
         for (int p = t.pb; ok && p < pe; ++p, ++q) {
-          const int ksteps = a.prs[p].ksteps;
+          const int ksteps = ks_next;
+          if (p + 1 < pe) ks_next = a.prs[p + 1].ksteps;
           const int buf = (int)(q & 1);
           if (!split_wait(&sm.tempty[buf], (unsigned)(((q >> 1) & 1) ^ 1), abort, g)) { ok = false; break; }
           tc_fence_after();
           const unsigned dbase = tmem + (unsigned)(buf * kBufCols);
           for (int ks = 0; ks < ksteps; ++ks, ++n) {
-            const int st = (int)(n % kSplitStages);
-            if (!split_wait(&sm.full[st], (unsigned)((n / kSplitStages) & 1), abort, g)) { ok = false; break; }
+            if (!split_wait(&sm.full[st], sph, abort, g)) { ok = false; break; }
             tc_fence_after();
             const signed char* a = sm.stage[st];
             const signed char* b = sm.stage[st] + a_bytes;
@@ -687,6 +693,10 @@ __global__ void __launch_bounds__(kSplitThreads, 1) k_split(const __grid_constan
                       idesc_i8(nn), (t == 1 && ks == 0) ? 0 : 1);
             }
             umma_commit(&sm.empty[st]);  // the stage is free once these MMAs have read it
+            if (++st == kSplitStages) {
+              st = 0;
+              sph ^= 1u;
+            }
           }
           if (!ok) break;
           umma_commit(&sm.tfull[buf]);  // the pair's groups are complete
@@ -994,9 +1004,18 @@ void split_records(sht_plan* p, cudaStream_t s) {
   trace("split: tile / pair records", s);
 }
 
-// One CTA per SM: it holds all 512 TMEM columns, and its shared memory keeps a second CTA off.
-constexpr size_t kSplitSmemLaunch = sizeof(SplitSmem);
-static_assert(kSplitSmemLaunch > 114 * 1024, "one split CTA per SM");
+// One CTA per SM: it holds all 512 TMEM columns, and its shared memory (at least 116 KB, more
+// than half an SM's) keeps a second CTA off.
+template <int S>
+constexpr size_t split_smem_bytes() {
+  return sizeof(SplitSmem<S>) > 116 * 1024 ? sizeof(SplitSmem<S>) : 116 * 1024;
+}
+static_assert(sizeof(SplitSmem<1>) <= kSplitSmemBudget && sizeof(SplitSmem<7>) <= kSplitSmemBudget &&
+                  sizeof(SplitSmem<8>) <= kSplitSmemBudget && split_stages(7) == 6,
+              "the split CTA's shared memory fits one SM");
+static const size_t kSplitSmemBytes[kMaxSlices] = {split_smem_bytes<1>(), split_smem_bytes<2>(), split_smem_bytes<3>(),
+                                                   split_smem_bytes<4>(), split_smem_bytes<5>(), split_smem_bytes<6>(),
+                                                   split_smem_bytes<7>(), split_smem_bytes<8>()};
 
 using SplitKernel = void (*)(SplitArgs);
 static const SplitKernel kSplitKernels[2][2][kMaxSlices] = {  // [multi][narrow][S - 1]
@@ -1027,10 +1046,11 @@ static int split_grid(sht_ctx* ctx) {
   std::call_once(once, [] {
     for (const auto& plane : kSplitKernels)
       for (const auto& row : plane)
-        for (SplitKernel k : row) {
-          SHT_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSplitSmemLaunch));
+        for (int si = 0; si < kMaxSlices; ++si) {
+          const SplitKernel k = row[si];
+          SHT_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSplitSmemBytes[si]));
           int n = 0;
-          SHT_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k, kSplitThreads, kSplitSmemLaunch));
+          SHT_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k, kSplitThreads, kSplitSmemBytes[si]));
           if (n != 1) fail(SHT_ERR_STATE, "split kernel must run one CTA per SM (TMEM budget)");
         }
   });
@@ -1099,7 +1119,7 @@ void split_launch(sht_plan* p, const SparseArgs& sa, cudaStream_t s) {
   const SplitArgs g = split_args(p, sa);
   if (g.nwork <= 0) return;
   const int grid = (int)std::min<long long>(split_grid(p->ctx), g.nwork);
-  kSplitKernels[0][split_narrow(p, g.S) ? 1 : 0][g.S - 1]<<<grid, kSplitThreads, kSplitSmemLaunch, s>>>(g);
+  kSplitKernels[0][split_narrow(p, g.S) ? 1 : 0][g.S - 1]<<<grid, kSplitThreads, kSplitSmemBytes[g.S - 1], s>>>(g);
   SHT_CUDA(cudaGetLastError());
   // an operand held a non-finite value (the slicer's flag): the tensor-core kernel returned at
   // once and the FP64 tiles compute the execute, with IEEE propagation as in the FP64 forms
@@ -1143,7 +1163,7 @@ long long split_multi_launch(sht_ctx* ctx, const std::vector<sht_plan*>& plans, 
   g.nmulti = (int)n;
   const int S = plans[0]->split_slices;
   const int grid = (int)std::min<long long>(split_grid(ctx), total);
-  kSplitKernels[1][kind & 1][S - 1]<<<grid, kSplitThreads, kSplitSmemLaunch, s>>>(g);
+  kSplitKernels[1][kind & 1][S - 1]<<<grid, kSplitThreads, kSplitSmemBytes[S - 1], s>>>(g);
   SHT_CUDA(cudaGetLastError());
   return total;
 }
