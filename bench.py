@@ -219,18 +219,25 @@ def cpu_leg(w, seconds: float, nthreads: int, ref: bool, runs: int):
 
 
 def count_launches(fn):
-    """Kernels launched by fn(), counted from the CUDA activity trace (CUPTI via torch)."""
+    """Kernels launched by fn(), counted from the CUDA activity trace (CUPTI via torch), and the
+    device time per kernel name (microseconds summed over its launches)."""
     import torch
     try:
         from torch.profiler import ProfilerActivity, profile
         with profile(activities=[ProfilerActivity.CUDA]) as prof:
             fn()
             torch.cuda.synchronize()
-        names = [e.name for e in prof.events() if e.device_type.name == "CUDA" and "memcpy" not in e.name.lower()
-                 and "memset" not in e.name.lower()]
-        return len(names), names
+        evs = [e for e in prof.events() if e.device_type.name == "CUDA" and "memcpy" not in e.name.lower()
+               and "memset" not in e.name.lower()]
+        per = {}
+        for e in evs:
+            key = e.name.split("(")[0].replace("void ", "")
+            n, us = per.get(key, (0, 0.0))
+            per[key] = (n + 1, us + float(e.time_range.elapsed_us()))
+        kernels = {k: {"launches": n, "us": round(us, 1)} for k, (n, us) in sorted(per.items(), key=lambda x: -x[1][1])}
+        return len(evs), kernels
     except Exception as ex:  # profiler unavailable
-        return None, [str(ex)]
+        return None, {"error": str(ex)}
 
 
 def measure_peak(sht, ctx, which):
@@ -729,7 +736,8 @@ def run_ours(args):
             "forms": results, "ratios": ratios, "split_slices_error": sweep or None, "oracle": oinfo,
             "roofline": roofline, "peaks": peaks, "cpu_baseline": cpu, "e2e": e2e, "clocks": clocks,
             "gpu_launches": (launches * args.steps) if launches is not None else None,
-            "gpu_launches_per_step": launches, "configs": configs or None, "serving": serving,
+            "gpu_launches_per_step": launches, "kernels_per_step": names or None,
+            "configs": configs or None, "serving": serving,
         }
         print(json.dumps(line), flush=True)
     ctx.close()
