@@ -620,11 +620,8 @@ __global__ void __launch_bounds__(kSplitThreads, 1) k_split(const __grid_constan
         bulk_g2s(sm.tile[is].rowoff, a.rowtab + t.rtab, 4 * kSplitM, &sm.ifull[is]);
         bulk_g2s(sm.tile[is].coloff, a.coltab + t.ctab, 4 * kSplitN, &sm.ifull[is]);
         const int pe = a.alpha_zero ? t.pb : t.pe;
-        // pair records one ahead: the load of the next is in flight while this pair's copies go out
-        SplitPair pr_next = t.pb < pe ? a.prs[t.pb] : SplitPair{};
         for (int p = t.pb; ok && p < pe; ++p, ++q) {
-          const SplitPair pr = pr_next;
-          if (p + 1 < pe) pr_next = a.prs[p + 1];
+          const SplitPair pr = a.prs[p];
           const int es = (int)(q % kExpSlots);
           if (!split_wait(&sm.eempty[es], (unsigned)(((q / kExpSlots) & 1) ^ 1), abort, g)) { ok = false; break; }
           mbar_expect_tx(&sm.efull[es], kExpSlotBytes);
@@ -671,10 +668,8 @@ __global__ void __launch_bounds__(kSplitThreads, 1) k_split(const __grid_constan
         if (a.flags_nonfinite) continue;
         const SplitItem t = a.items[li];
         const int pe = a.alpha_zero ? t.pb : t.pe;
-        int ks_next = t.pb < pe ? a.prs[t.pb].ksteps : 0;  // one pair ahead, as the producer
         for (int p = t.pb; ok && p < pe; ++p, ++q) {
-          const int ksteps = ks_next;
-          if (p + 1 < pe) ks_next = a.prs[p + 1].ksteps;
+          const int ksteps = a.prs[p].ksteps;
           const int buf = (int)(q & 1);
           if (!split_wait(&sm.tempty[buf], (unsigned)(((q >> 1) & 1) ^ 1), abort, g)) { ok = false; break; }
           tc_fence_after();
