@@ -64,7 +64,9 @@ constexpr int kBufCols = kMaxSlices * kSplitN;  // TMEM columns of one accumulat
 constexpr int kSplitTmemCols = 2 * kBufCols;    // two sets: 512 columns, the whole TMEM of an SM
 constexpr int kEpiWarps = 16;                   // 4 TMEM lane quarters x 4 column quarters
 constexpr int kTileSlots = 4, kExpSlots = 4;    // depth of the tile-record and exponent rings
-constexpr int kSplitThreads = 64 + kEpiWarps * 32;
+constexpr int kRecSlots = 16;                   // depth of the record ring (power of two)
+constexpr int kRecWarp = 2 + kEpiWarps;         // the record warp, after the epilogue warps
+constexpr int kSplitThreads = 64 + kEpiWarps * 32 + 32;
 
 // ------------------------------------------------------------------ slicing
 
@@ -424,6 +426,22 @@ struct SplitArgs {
 // ring of tile slots, and per pair the A row exponents, the B column exponents and the B
 // column scales into a ring of exponent slots, so the epilogue reads nothing from global
 // memory but the C values it scales by beta.
+// One record of the producer's and the MMA issuer's work stream: one pair of one tile (or a
+// tile without pairs), its copy sources resolved by the record warp.
+struct SplitRec {
+  const signed char* a_src;  // A slabs of the pair's k-steps for the tile's rows
+  const signed char* b_src;  // B slabs for the tile's columns
+  const short* ae_src;
+  const short* be_src;
+  const double* bsc_src;
+  const SplitItem* rec_src;  // the tile record, its row and column offsets (first record of a tile)
+  const int* rowtab_src;
+  const int* coltab_src;
+  int ksteps;                // 0: a tile without pairs
+  int kind;                  // kRecFirst: first record of its tile; kRecEnd: end of the stream
+};
+constexpr int kRecFirst = 1, kRecEnd = 4;
+
 struct SplitTileSlot {
   SplitItem rec;
   int rowoff[kSplitM];
@@ -448,6 +466,8 @@ struct SplitSmem {
   alignas(16) SplitExpSlot ex[kExpSlots];
   alignas(8) unsigned long long full[kStages], empty[kStages], tfull[2], tempty[2], drain;
   unsigned long long ifull[kTileSlots], iempty[kTileSlots], efull[kExpSlots], eempty[kExpSlots];
+  unsigned long long rfull[kRecSlots], rempty[kRecSlots];
+  SplitRec rec[kRecSlots];
   unsigned tmem_base;
   int abort;
 };
@@ -590,6 +610,10 @@ __global__ void __launch_bounds__(kSplitThreads, 1) k_split(const __grid_constan
       mbar_init(&sm.efull[i], 1);
       mbar_init(&sm.eempty[i], kEpiWarps);
     }
+    for (int i = 0; i < kRecSlots; ++i) {
+      mbar_init(&sm.rfull[i], 1);
+      mbar_init(&sm.rempty[i], 2);  // the producer and the MMA issuer
+    }
     mbar_init(&sm.drain, 1);
     sm.abort = 0;
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
@@ -607,39 +631,41 @@ __global__ void __launch_bounds__(kSplitThreads, 1) k_split(const __grid_constan
       int st = 0;         // stage of k-step n (n % kSplitStages) and its ring phase
       unsigned sph = 0;
       bool ok = true;
-      for (int item = blockIdx.x; ok && item < g.nwork; item += gridDim.x) {
-        int li;
-        const SplitReq a = split_req<Multi>(g, item, li);
-        if (a.flags_nonfinite) continue;
-        const SplitItem t = a.items[li];
-        const int is = (int)(ni % kTileSlots);
-        if (!split_wait(&sm.iempty[is], (unsigned)(((ni / kTileSlots) & 1) ^ 1), abort, g)) { ok = false; break; }
-        ++ni;
-        mbar_expect_tx(&sm.ifull[is], kTileSlotBytes);
-        bulk_g2s(&sm.tile[is].rec, a.items + li, sizeof(SplitItem), &sm.ifull[is]);
-        bulk_g2s(sm.tile[is].rowoff, a.rowtab + t.rtab, 4 * kSplitM, &sm.ifull[is]);
-        bulk_g2s(sm.tile[is].coloff, a.coltab + t.ctab, 4 * kSplitN, &sm.ifull[is]);
-        const int pe = a.alpha_zero ? t.pb : t.pe;
-        for (int p = t.pb; ok && p < pe; ++p, ++q) {
-          const SplitPair pr = a.prs[p];
-          const int es = (int)(q % kExpSlots);
-          if (!split_wait(&sm.eempty[es], (unsigned)(((q / kExpSlots) & 1) ^ 1), abort, g)) { ok = false; break; }
-          mbar_expect_tx(&sm.efull[es], kExpSlotBytes);
-          bulk_g2s(sm.ex[es].ea, a.Ae + pr.ae_off + t.r0, 2 * kSplitM, &sm.efull[es]);
-          bulk_g2s(sm.ex[es].eb, a.Be + pr.be_off + t.c0, 2 * kSplitN, &sm.efull[es]);
-          bulk_g2s(sm.ex[es].sc, a.Bsc + pr.be_off + t.c0, 8 * kSplitN, &sm.efull[es]);
-          const int ksteps = pr.ksteps;
-          const signed char* asrc = a.As + pr.a_off + (long long)(t.r0 / kSplitM) * ksteps * a_bytes;
-          const signed char* bsrc = a.Bs + pr.b_off + (long long)(t.c0 / kSplitN) * ksteps * b_bytes;
-          for (int ks = 0; ks < ksteps; ++ks, ++n) {
-            if (!split_wait(&sm.empty[st], sph ^ 1u, abort, g)) { ok = false; break; }
-            mbar_expect_tx(&sm.full[st], a_bytes + b_bytes);
-            bulk_g2s(sm.stage[st], asrc + (long long)ks * a_bytes, a_bytes, &sm.full[st]);
-            bulk_g2s(sm.stage[st] + a_bytes, bsrc + (long long)ks * b_bytes, b_bytes, &sm.full[st]);
-            if (++st == kSplitStages) {
-              st = 0;
-              sph ^= 1u;
-            }
+      for (long long r = 0; ok; ++r) {
+        const int rs = (int)(r & (kRecSlots - 1));
+        if (!split_wait(&sm.rfull[rs], (unsigned)((r / kRecSlots) & 1), abort, g)) { ok = false; break; }
+        const SplitRec v = sm.rec[rs];
+        mbar_arrive(&sm.rempty[rs]);
+        if (v.kind & kRecEnd) break;
+        if (v.kind & kRecFirst) {
+          const int is = (int)(ni % kTileSlots);
+          if (!split_wait(&sm.iempty[is], (unsigned)(((ni / kTileSlots) & 1) ^ 1), abort, g)) { ok = false; break; }
+          ++ni;
+          mbar_expect_tx(&sm.ifull[is], kTileSlotBytes);
+          bulk_g2s(&sm.tile[is].rec, v.rec_src, sizeof(SplitItem), &sm.ifull[is]);
+          bulk_g2s(sm.tile[is].rowoff, v.rowtab_src, 4 * kSplitM, &sm.ifull[is]);
+          bulk_g2s(sm.tile[is].coloff, v.coltab_src, 4 * kSplitN, &sm.ifull[is]);
+        }
+        if (v.ksteps == 0) continue;
+        const int es = (int)(q % kExpSlots);
+        if (!split_wait(&sm.eempty[es], (unsigned)(((q / kExpSlots) & 1) ^ 1), abort, g)) { ok = false; break; }
+        ++q;
+        mbar_expect_tx(&sm.efull[es], kExpSlotBytes);
+        bulk_g2s(sm.ex[es].ea, v.ae_src, 2 * kSplitM, &sm.efull[es]);
+        bulk_g2s(sm.ex[es].eb, v.be_src, 2 * kSplitN, &sm.efull[es]);
+        bulk_g2s(sm.ex[es].sc, v.bsc_src, 8 * kSplitN, &sm.efull[es]);
+        const signed char* asrc = v.a_src;
+        const signed char* bsrc = v.b_src;
+        for (int ks = 0; ks < v.ksteps; ++ks, ++n) {
+          if (!split_wait(&sm.empty[st], sph ^ 1u, abort, g)) { ok = false; break; }
+          mbar_expect_tx(&sm.full[st], a_bytes + b_bytes);
+          bulk_g2s(sm.stage[st], asrc, a_bytes, &sm.full[st]);
+          bulk_g2s(sm.stage[st] + a_bytes, bsrc, b_bytes, &sm.full[st]);
+          asrc += a_bytes;
+          bsrc += b_bytes;
+          if (++st == kSplitStages) {
+            st = 0;
+            sph ^= 1u;
           }
         }
       }
@@ -662,44 +688,109 @@ __global__ void __launch_bounds__(kSplitThreads, 1) k_split(const __grid_constan
       int st = 0;  // stage of k-step n and its ring phase, as the producer's
       unsigned sph = 0;
       bool ok = true;
-      for (int item = blockIdx.x; ok && item < g.nwork; item += gridDim.x) {
-        int li;
-        const SplitReq a = split_req<Multi>(g, item, li);
-        if (a.flags_nonfinite) continue;
-        const SplitItem t = a.items[li];
-        const int pe = a.alpha_zero ? t.pb : t.pe;
-        for (int p = t.pb; ok && p < pe; ++p, ++q) {
-          const int ksteps = a.prs[p].ksteps;
-          const int buf = (int)(q & 1);
-          if (!split_wait(&sm.tempty[buf], (unsigned)(((q >> 1) & 1) ^ 1), abort, g)) { ok = false; break; }
+      for (long long r = 0; ok; ++r) {
+        const int rs = (int)(r & (kRecSlots - 1));
+        if (!split_wait(&sm.rfull[rs], (unsigned)((r / kRecSlots) & 1), abort, g)) { ok = false; break; }
+        const int ksteps = sm.rec[rs].ksteps, kind = sm.rec[rs].kind;
+        mbar_arrive(&sm.rempty[rs]);
+        if (kind & kRecEnd) break;
+        if (ksteps == 0) continue;
+        const int buf = (int)(q & 1);
+        if (!split_wait(&sm.tempty[buf], (unsigned)(((q >> 1) & 1) ^ 1), abort, g)) { ok = false; break; }
+        ++q;
+        tc_fence_after();
+        const unsigned dbase = tmem + (unsigned)(buf * kBufCols);
+        for (int ks = 0; ks < ksteps; ++ks, ++n) {
+          if (!split_wait(&sm.full[st], sph, abort, g)) { ok = false; break; }
           tc_fence_after();
-          const unsigned dbase = tmem + (unsigned)(buf * kBufCols);
-          for (int ks = 0; ks < ksteps; ++ks, ++n) {
-            if (!split_wait(&sm.full[st], sph, abort, g)) { ok = false; break; }
-            tc_fence_after();
-            const signed char* a = sm.stage[st];
-            const signed char* b = sm.stage[st] + a_bytes;
-            // A slice t times B slices 1..S+1-t in one MMA: the products land in TMEM groups
-            // g = t+1 .. S+1, i.e. columns from (t-1)*32 on; t = 1 writes every group first.
+          const signed char* a = sm.stage[st];
+          const signed char* b = sm.stage[st] + a_bytes;
+          // A slice t times B slices 1..S+1-t in one MMA: the products land in TMEM groups
+          // g = t+1 .. S+1, i.e. columns from (t-1)*32 on; t = 1 writes every group first.
 #pragma unroll
-            for (int t = 1; t <= S; ++t) {
-              const int nn = kSplitN * (S + 1 - t);
-              umma_i8(dbase + (unsigned)((t - 1) * kSplitN), umma_desc(a + (t - 1) * kAChunk), umma_desc(b),
-                      idesc_i8(nn), (t == 1 && ks == 0) ? 0 : 1);
-            }
-            umma_commit(&sm.empty[st]);  // the stage is free once these MMAs have read it
-            if (++st == kSplitStages) {
-              st = 0;
-              sph ^= 1u;
-            }
+          for (int t = 1; t <= S; ++t) {
+            const int nn = kSplitN * (S + 1 - t);
+            umma_i8(dbase + (unsigned)((t - 1) * kSplitN), umma_desc(a + (t - 1) * kAChunk), umma_desc(b),
+                    idesc_i8(nn), (t == 1 && ks == 0) ? 0 : 1);
           }
-          if (!ok) break;
-          umma_commit(&sm.tfull[buf]);  // the pair's groups are complete
+          umma_commit(&sm.empty[st]);  // the stage is free once these MMAs have read it
+          if (++st == kSplitStages) {
+            st = 0;
+            sph ^= 1u;
+          }
         }
+        if (!ok) break;
+        umma_commit(&sm.tfull[buf]);  // the pair's groups are complete
       }
       // drain: every MMA issued above has finished before TMEM is released (bounded)
       umma_commit(&sm.drain);
       split_settle(&sm.drain, 0, g);
+    }
+    __syncwarp();
+  } else if (warp == kRecWarp) {
+    // ---------------------------------------------------------------- record warp
+    // Walks the CTA's tiles 32 at a time, one tile per lane: the lanes load their tile records
+    // and first pair records in parallel, then write their records into the ring in stream order
+    // (lane after lane), resolving every copy source, so that the producer and the MMA issuer
+    // read their work from shared memory.  Ends the stream with a kRecEnd record.
+    long long r = 0;  // records written
+    bool ok = true;
+    for (int base = blockIdx.x; ok && base < g.nwork; base += 32 * gridDim.x) {
+      const int item = base + lane * gridDim.x;
+      int li = 0;
+      SplitItem t{};
+      SplitReq a{};
+      int np = 0, cnt = 0;
+      if (item < g.nwork) {
+        a = split_req<Multi>(g, item, li);
+        if (!a.flags_nonfinite) {
+          t = a.items[li];
+          np = a.alpha_zero ? 0 : t.pe - t.pb;
+          cnt = np > 0 ? np : 1;
+        }
+      }
+      SplitPair pr{};
+      if (np > 0) pr = a.prs[t.pb];
+      for (int l = 0; ok && l < 32; ++l) {
+        const int c = __shfl_sync(0xffffffffu, cnt, l);
+        if (lane == l) {
+          for (int j = 0; ok && j < c; ++j, ++r) {
+            if (j > 0) pr = a.prs[t.pb + j];
+            const int rs = (int)(r & (kRecSlots - 1));
+            if (!split_wait(&sm.rempty[rs], (unsigned)(((r / kRecSlots) & 1) ^ 1), abort, g)) { ok = false; break; }
+            SplitRec v;
+            v.kind = j == 0 ? kRecFirst : 0;
+            v.rec_src = a.items + li;
+            v.rowtab_src = a.rowtab + t.rtab;
+            v.coltab_src = a.coltab + t.ctab;
+            if (np > 0) {
+              v.ksteps = pr.ksteps;
+              v.a_src = a.As + pr.a_off + (long long)(t.r0 / kSplitM) * pr.ksteps * a_bytes;
+              v.b_src = a.Bs + pr.b_off + (long long)(t.c0 / kSplitN) * pr.ksteps * b_bytes;
+              v.ae_src = a.Ae + pr.ae_off + t.r0;
+              v.be_src = a.Be + pr.be_off + t.c0;
+              v.bsc_src = a.Bsc + pr.be_off + t.c0;
+            } else {
+              v.ksteps = 0;
+              v.a_src = v.b_src = nullptr;
+              v.ae_src = v.be_src = nullptr;
+              v.bsc_src = nullptr;
+            }
+            sm.rec[rs] = v;
+            mbar_arrive(&sm.rfull[rs]);  // release: the record's stores come first
+          }
+        }
+        r = __shfl_sync(0xffffffffu, r, l);
+        ok = __shfl_sync(0xffffffffu, ok ? 1 : 0, l) != 0;
+      }
+    }
+    if (ok && lane == 0) {
+      const int rs = (int)(r & (kRecSlots - 1));
+      if (split_wait(&sm.rempty[rs], (unsigned)(((r / kRecSlots) & 1) ^ 1), abort, g)) {
+        sm.rec[rs].kind = kRecEnd;
+        sm.rec[rs].ksteps = 0;
+        mbar_arrive(&sm.rfull[rs]);
+      }
     }
     __syncwarp();
   } else {
