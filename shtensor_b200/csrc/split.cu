@@ -20,16 +20,19 @@
 // (cp.async.bulk, completion counted on an mbarrier).  The B slabs of one k-step lie one
 // after another, so slices u = 1..n together form one operand of 32*n columns.
 //
-// Kernel (k_split, one 576-thread CTA per SM, persistent over 128 x 32 tiles of C):
+// Kernel (k_split, one 384-thread CTA per SM, persistent over 128 x 32 tiles of C):
 //   warp 0      producer: for every (tile, pair, k-step) waits for a free stage of the
-//               4-stage shared-memory ring and issues its two bulk copies;
+//               shared-memory ring (split_stages(S) deep) and issues its two bulk copies;
 //   warp 1      MMA issuer: waits for the stage and issues S MMAs, A slice t times B slices
 //               1..S+1-t (N = 32*(S+1-t)) into TMEM groups t+1..S+1 of one of two
 //               accumulator sets; frees the stage with tcgen05.commit and, at the end of a
 //               pair, commits the accumulator set to the epilogue;
-//   warps 2-17  epilogue: 4 TMEM lane quarters x 4 column quarters of 8 columns; reassemble a
+//   warps 2-9   epilogue: 4 TMEM lane quarters x 2 column halves of 16 columns; reassemble a
 //               pair's groups while the tensor cores already work on the next pair (second
-//               TMEM set), accumulate in registers, store the tile at the end.
+//               TMEM set), accumulate in registers, store the tile at the end;
+//   warp 10     record warp: resolves each pair's copy sources and exponent rows into a
+//               shared ring that the producer and the MMA issuer read;
+//   warp 11     idle (it only lifts the register allowance to 168 per thread).
 // Per-tile and per-pair records are built at plan time so that each role reads one record
 // per tile and per pair.  Every wait is bounded: a role that gives up raises a CTA-wide abort
 // flag and the error word (SHT_ERR_TIMEOUT); the others leave their waits on the flag, the
@@ -62,11 +65,15 @@ constexpr int kAChunk = kSplitM * kSplitK;      // bytes of one A slab (128 rows
 constexpr int kBChunk = kSplitN * kSplitK;      // bytes of one B slab (32 columns x 32 k)
 constexpr int kBufCols = kMaxSlices * kSplitN;  // TMEM columns of one accumulator set (8 groups)
 constexpr int kSplitTmemCols = 2 * kBufCols;    // two sets: 512 columns, the whole TMEM of an SM
-constexpr int kEpiWarps = 16;                   // 4 TMEM lane quarters x 4 column quarters
+constexpr int kEpiWarps = 8;                    // 4 TMEM lane quarters x (kEpiWarps / 4) column parts
+constexpr int kEpiCols = kSplitN / (kEpiWarps / 4);  // tile columns per epilogue thread
 constexpr int kTileSlots = 4, kExpSlots = 4;    // depth of the tile-record and exponent rings
 constexpr int kRecSlots = 16;                   // depth of the record ring (power of two)
 constexpr int kRecWarp = 2 + kEpiWarps;         // the record warp, after the epilogue warps
-constexpr int kSplitThreads = 64 + kEpiWarps * 32 + 32;
+// 12 warps: producer, MMA issuer, 8 epilogue warps, record warp, one idle warp.  Twelve warps
+// put three on each SM sub-partition, whose 16K registers then allow 168 per thread (eleven
+// would allow only 160 per thread under the launch bound's rounding).
+constexpr int kSplitThreads = 64 + kEpiWarps * 32 + 64;
 
 // ------------------------------------------------------------------ slicing
 
@@ -237,6 +244,20 @@ __device__ __forceinline__ void mbar_init(void* mbar, unsigned count) {
   asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(mbar)), "r"(count) : "memory");
 }
 
+__device__ __forceinline__ void tmem_ld16(unsigned taddr, unsigned* v) {
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];\n"
+      : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]), "=r"(v[8]),
+        "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
+      : "r"(taddr)
+      : "memory");
+}
+__device__ __forceinline__ void tmem_ld8(unsigned taddr, unsigned* v);
+// kEpiCols consecutive TMEM columns of this warp's 32 lanes into v
+__device__ __forceinline__ void tmem_ldc(unsigned taddr, unsigned* v) {
+  if constexpr (kEpiCols == 16) tmem_ld16(taddr, v);
+  else tmem_ld8(taddr, v);
+}
 __device__ __forceinline__ void tmem_ld8(unsigned taddr, unsigned* v) {
   asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];\n"
                : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7])
@@ -546,15 +567,15 @@ __host__ __device__ constexpr int narrow_wexp(int S, int k) { return S == 1 ? -1
 // Loads groups [g0, g1) of this thread's 8 columns from TMEM and folds them into the narrow
 // sums X (groups 2k and 2k+1 into X_k; the odd last group rounded into X_(nx-1)).
 template <int S, int g0, int g1>
-__device__ __forceinline__ void narrow_load(unsigned tb, int (&X)[narrow_nx(S)][8]) {
-  unsigned v[g1 - g0][8];
+__device__ __forceinline__ void narrow_load(unsigned tb, int (&X)[narrow_nx(S)][kEpiCols]) {
+  unsigned v[g1 - g0][kEpiCols];
 #pragma unroll
-  for (int i = 0; i < g1 - g0; ++i) tmem_ld8(tb + (unsigned)((g0 + i) * kSplitN), v[i]);
+  for (int i = 0; i < g1 - g0; ++i) tmem_ldc(tb + (unsigned)((g0 + i) * kSplitN), v[i]);
   tmem_wait_ld();
 #pragma unroll
   for (int gi = g0; gi < g1; ++gi) {
 #pragma unroll
-    for (int j = 0; j < 8; ++j) {
+    for (int j = 0; j < kEpiCols; ++j) {
       const int p = (int)v[gi - g0][j];
       if (S == 1) {
         X[0][j] = p;
@@ -793,7 +814,7 @@ __global__ void __launch_bounds__(kSplitThreads, 1) k_split(const __grid_constan
       }
     }
     __syncwarp();
-  } else {
+  } else if (warp < 2 + kEpiWarps) {
     // ---------------------------------------------------------------- epilogue
     const int quarter = warp & 3, cq = (warp - 2) >> 2;
     const int row = quarter * 32 + lane;  // the TMEM lane this warp may read
@@ -813,21 +834,21 @@ __global__ void __launch_bounds__(kSplitThreads, 1) k_split(const __grid_constan
       const SplitItem t = ts.rec;
       const bool row_in = row < t.mt;
       // a warp whose rows or columns all lie outside a partial tile skips the reassembly
-      const bool warp_live = quarter * 32 < t.mt && cq * 8 < t.nt;
+      const bool warp_live = quarter * 32 < t.mt && cq * kEpiCols < t.nt;
       const int roff = ts.rowoff[row];
-      int coff[8];
+      int coff[kEpiCols];
 #pragma unroll
-      for (int j = 0; j < 8; ++j) coff[j] = ts.coloff[cq * 8 + j];
+      for (int j = 0; j < kEpiCols; ++j) coff[j] = ts.coloff[cq * kEpiCols + j];
       // the slot is refilled by the async proxy (bulk copy): order this warp's generic reads
       // of it before the release (write-after-read across proxies needs the proxy fence)
       fence_proxy_async_smem();
       __syncwarp();
       if (lane == 0) mbar_arrive(&sm.iempty[is]);
       double* cptr = a.C + t.cbase;
-      double acc[8];
+      double acc[kEpiCols];
 #pragma unroll
-      for (int j = 0; j < 8; ++j) {
-        const bool in = row_in && cq * 8 + j < t.nt;
+      for (int j = 0; j < kEpiCols; ++j) {
+        const bool in = row_in && cq * kEpiCols + j < t.nt;
         acc[j] = (a.beta_zero || !in) ? 0.0 : __dmul_rn(a.beta, cptr[roff + coff[j]]);
       }
       const int pe = a.alpha_zero ? t.pb : t.pe;
@@ -843,8 +864,8 @@ __global__ void __launch_bounds__(kSplitThreads, 1) k_split(const __grid_constan
         // the slot's exponents and column scales are read where they are used; the slot is
         // released after the pair's arithmetic (the ring is four deep)
         const SplitExpSlot& ex = sm.ex[es];
-        const double* sc = &ex.sc[cq * 8];
-        const short* fe = &ex.eb[cq * 8];
+        const double* sc = &ex.sc[cq * kEpiCols];
+        const short* fe = &ex.eb[cq * kEpiCols];
         const int er = ex.ea[row];
         auto release_exp = [&]() {
           fence_proxy_async_smem();  // as for the tile slot
@@ -852,7 +873,7 @@ __global__ void __launch_bounds__(kSplitThreads, 1) k_split(const __grid_constan
           if (lane == 0) mbar_arrive(&sm.eempty[es]);
         };
         tc_fence_after();
-        const unsigned tb = tmem + tlane + (unsigned)(buf * kBufCols + cq * 8);
+        const unsigned tb = tmem + tlane + (unsigned)(buf * kBufCols + cq * kEpiCols);
         auto release_set = [&]() {
           // the groups are in registers: the accumulator set may be overwritten
           tc_fence_before();
@@ -867,7 +888,7 @@ __global__ void __launch_bounds__(kSplitThreads, 1) k_split(const __grid_constan
         if constexpr (Narrow) {
           // ---- narrow: NX 32-bit sums, one conversion each
           constexpr int NX = narrow_nx(S);
-          int X[NX][8];
+          int X[NX][kEpiCols];
           narrow_load<S, 0, (S < 4 ? S : 4)>(tb, X);
           if constexpr (S > 4) narrow_load<S, 4, S>(tb, X);
           release_set();
@@ -879,7 +900,7 @@ __global__ void __launch_bounds__(kSplitThreads, 1) k_split(const __grid_constan
             for (int k = 0; k < NX; ++k) W[k] = pow2(er + narrow_wexp(S, k));
             const double mlast = -kM * W[NX - 1];
 #pragma unroll
-            for (int j = 0; j < 8; ++j) {
+            for (int j = 0; j < kEpiCols; ++j) {
               // smallest weight first; the first product is exact: (2^52 + 2^31 + X) W - (2^52 + 2^31) W
               double part = fma(__hiloint2double(0x43300000, X[NX - 1][j] ^ (int)0x80000000), W[NX - 1], mlast);
 #pragma unroll
@@ -889,7 +910,7 @@ __global__ void __launch_bounds__(kSplitThreads, 1) k_split(const __grid_constan
             }
           } else {
 #pragma unroll
-            for (int j = 0; j < 8; ++j) {
+            for (int j = 0; j < kEpiCols; ++j) {
               double part = 0.0;
 #pragma unroll
               for (int k = NX - 1; k >= 0; --k)
@@ -903,24 +924,24 @@ __global__ void __launch_bounds__(kSplitThreads, 1) k_split(const __grid_constan
           // ---- wide: the INT32 groups are combined exactly in int64 three at a time
           // (P_g 2^14 + P_g+1 2^7 + P_g+2 < 2^46), each triple converted once and weighted by
           // an exact power of two (smallest weights first)
-          double part[8];
+          double part[kEpiCols];
 #pragma unroll
-          for (int j = 0; j < 8; ++j) part[j] = 0.0;
+          for (int j = 0; j < kEpiCols; ++j) part[j] = 0.0;
 #pragma unroll
           for (int c = (kMaxSlices - 1) / 3; c >= 0; --c) {
             const int g0 = 3 * c;
             if (g0 >= S) continue;
             const int len = min(3, S - g0);
-            unsigned v[3][8];
+            unsigned v[3][kEpiCols];
 #pragma unroll
             for (int i = 0; i < 3; ++i)
-              if (i < len) tmem_ld8(tb + (unsigned)((g0 + i) * kSplitN), v[i]);
+              if (i < len) tmem_ldc(tb + (unsigned)((g0 + i) * kSplitN), v[i]);
             tmem_wait_ld();
             if (c == 0) release_set();
             // the triple's lowest group has weight 2^(-7(g0 + len - 1)) relative to group 2
             const double w = pow2(-7 * (g0 + len - 1));
 #pragma unroll
-            for (int j = 0; j < 8; ++j) {
+            for (int j = 0; j < kEpiCols; ++j) {
               long long x = (int)v[0][j];
               if (len > 1) x = x * 128 + (int)v[1][j];
               if (len > 2) x = x * 128 + (int)v[2][j];
@@ -931,10 +952,10 @@ __global__ void __launch_bounds__(kSplitThreads, 1) k_split(const __grid_constan
             // part * 2^(e_r - 14) is exact (normal) and sc[j] = 2^(f_c): one rounding
             const double sr = pow2(er - 14);
 #pragma unroll
-            for (int j = 0; j < 8; ++j) acc[j] = fma(part[j] * sr, sc[j], acc[j]);
+            for (int j = 0; j < kEpiCols; ++j) acc[j] = fma(part[j] * sr, sc[j], acc[j]);
           } else {
 #pragma unroll
-            for (int j = 0; j < 8; ++j) {
+            for (int j = 0; j < kEpiCols; ++j) {
               const int e = er + fe[j] - 14;
               acc[j] = (e >= -1022 && e <= 1023) ? fma(part[j], pow2(e), acc[j]) : acc[j] + scalbn(part[j], e);
             }
@@ -945,8 +966,8 @@ __global__ void __launch_bounds__(kSplitThreads, 1) k_split(const __grid_constan
       if (!ok) break;
       if (row_in) {
 #pragma unroll
-        for (int j = 0; j < 8; ++j)
-          if (cq * 8 + j < t.nt) cptr[roff + coff[j]] = acc[j];
+        for (int j = 0; j < kEpiCols; ++j)
+          if (cq * kEpiCols + j < t.nt) cptr[roff + coff[j]] = acc[j];
       }
     }
   }
