@@ -92,123 +92,295 @@ __host__ __device__ __forceinline__ int slab_offset(int r, int k) {
 constexpr int kFlagNonFinite = 0, kFlagGeneralExp = 1;
 constexpr int kExpLoA = -900, kExpHiA = 960, kExpLoB = -1022, kExpHiB = 1023;
 
-// One 128-thread CTA per item of 32 rows of one block (items are numbered block after block,
-// istart[b] the first item of block b).  Lane = row; warp w takes the 16-wide k-chunks w, w+4,
-// ... of the row (a warp's load of one k is 32 consecutive rows of a column-major block).  The
-// chunk of each warp stays in registers when K <= 64 (one chunk per warp); the row maximum is
-// reduced over the four warps in shared memory and gives the row's exponent (rows padded up to
-// the tile height R get 0); then every chunk is cut into its S int8 slices, packed four bytes
-// to a register and stored as one 16-byte word per slice, in tile order:
+// One operand of the slicer: A (rows = A's free modes, tiles of 128 rows, alpha folded into the
+// values) or B (rows = B's free modes, i.e. C columns, tiles of 32 rows, column scales written).
+struct SliceOperand {
+  const double* src;           // the operand's block data
+  const long long* src_off;    // element offset of every block
+  const int* dims;             // block extents, order per block
+  const long long* out_off;    // byte offset of every block's slices
+  const long long* exp_off;    // offset of every block's row exponents
+  const long long* istart;     // first slicer item of every block (items of 32 rows)
+  signed char* out;
+  short* expo;
+  double* pscale;              // B: 2^e per column (0 when e is outside [elo, ehi]); A: null
+  double scale;
+  long long nblocks, nitems;
+  ModeMap fm, km;              // the row modes and the contracted modes
+  int order, R, elo, ehi;
+};
+struct SliceArgs {
+  SliceOperand op[2];          // A, then B: items of A first, then items of B
+  int* flags;
+};
+
+// The block holding item it: the last b with istart[b] <= it (istart[0] = 0, non-decreasing),
+// found by the warp 32 ways at a time (two dependent loads for up to 1024 blocks).
+__device__ __forceinline__ long long item_block(const long long* __restrict__ istart, long long nblocks, long long it,
+                                                int lane) {
+  long long lo = 0, n = nblocks;  // invariant: istart[lo] <= it, and lo + n == nblocks or istart[lo + n] > it
+  while (n > 1) {
+    const long long step = (n + 31) >> 5;
+    const long long off = (long long)lane * step;
+    const bool le = off < n && __ldg(istart + lo + off) <= it;
+    const int last = 31 - __clz(__ballot_sync(0xffffffffu, le));  // lane 0 (off 0) always holds
+    lo += (long long)last * step;
+    n = min(step, n - (long long)last * step);
+  }
+  return lo;
+}
+
+// d = bytes of {b, a} chosen by the selector nibbles of c; a nibble with bit 3 set gives the
+// sign of its byte replicated over 8 bits
+__device__ __forceinline__ unsigned prmt(unsigned a, unsigned b, unsigned c) {
+  unsigned d;
+  asm("prmt.b32 %0, %1, %2, %3;" : "=r"(d) : "r"(a), "r"(b), "r"(c));
+  return d;
+}
+
+// 8-byte global -> shared copy (cp.async), zero-filled when bytes is 0
+__device__ __forceinline__ void cp_async8(void* smem, const void* gmem, int bytes) {
+  const unsigned sa = static_cast<unsigned>(__cvta_generic_to_shared(smem));
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(sa), "l"(gmem), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit8() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait8() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
+
+// offset of index idx of the modes mm within a block of extents d and strides st
+__device__ __forceinline__ int mode_offset(const int* d, const int* st, const ModeMap& mm, int idx) {
+  int off = 0;
+  for (int t = 0; t < mm.n; ++t) {
+    const int e = d[mm.x[t]];
+    off += (idx % e) * st[mm.x[t]];
+    idx /= e;
+  }
+  return off;
+}
+
+// Where one slicer item lies: its operand, its block (and the block's item range), the block's
+// extents, and this lane's row in the block.
+struct SliceLoc {
+  long long b, bstart, bend;
+  int opb, m, K, r;
+};
+
+// The location of item `item` (items of A first, then of B).  A CTA walks a contiguous range of
+// items, so the block of the previous item (prev) is reused while the item stays inside it.
+__device__ __forceinline__ SliceLoc slice_locate(const SliceArgs& g, long long item, const SliceLoc& prev, int lane) {
+  const long long na = g.op[0].nitems;
+  const int opb = item >= na ? 1 : 0;
+  const SliceOperand& o = g.op[opb];
+  const long long it = opb ? item - na : item;
+  SliceLoc L;
+  if (prev.opb == opb && it >= prev.bstart && it < prev.bend) {
+    L = prev;
+  } else {
+    L.opb = opb;
+    L.b = item_block(o.istart, o.nblocks, it, lane);
+    L.bstart = o.istart[L.b];
+    L.bend = L.b + 1 < o.nblocks ? o.istart[L.b + 1] : o.nitems;
+    const int* d = o.dims + L.b * o.order;
+    int m = 1, K = 1;
+    for (int t = 0; t < o.fm.n; ++t) m *= d[o.fm.x[t]];
+    for (int t = 0; t < o.km.n; ++t) K *= d[o.km.x[t]];
+    L.m = m;
+    L.K = K;
+  }
+  L.r = (int)(it - L.bstart) * 32 + lane;
+  return L;
+}
+
+// Slices t = 1..S of the 8 values v (|v| * 2^-e < 1) of one row and one 8-wide k-chunk,
+// stored as one 8-byte word per slice at out + base + (t - 1) * slab.  z = 1 + |y|, y = v 2^-e,
+// rounded toward zero holds |y|'s first 52 bits in its mantissa, so slice t (t <= 7) is the
+// 7-bit field of fraction bits 7t-6 .. 7t, negated when v is negative: exactly the digits of
+// repeated s_t = trunc(128 * remainder).  Slice 8 takes fraction bits 50..52 from z and
+// 53..56 from the exact tail |y| - (z - 1).  Four slices are packed into a register by byte
+// permutes and negated four bytes at once ((0x80 - b) ^ 0x80 = -b mod 256 for 0 <= b <= 127,
+// with no carry between bytes).
+template <int S>
+__device__ __forceinline__ void slice_chunk(const double (&v)[8], int e, signed char* out, long long base,
+                                            long long slab) {
+  // |v| * 2^-e is exact when 2^-e is a normal double and the product is normal; a product
+  // below 2^-1022 has only zero slices either way.  Other exponents scale with scalbn.
+  const bool mul = e >= -1022 && e <= 1022;
+  const double inv = mul ? __longlong_as_double((long long)(1023 - e) << 52) : 0.0;
+  unsigned w[S][2];
+#pragma unroll
+  for (int q = 0; q < 2; ++q) {
+    // byte masks of the four values' signs: 0xff where negative
+    const unsigned sm = prmt(prmt((unsigned)__double2hiint(v[4 * q]), (unsigned)__double2hiint(v[4 * q + 1]), 0x00fbu),
+                             prmt((unsigned)__double2hiint(v[4 * q + 2]), (unsigned)__double2hiint(v[4 * q + 3]), 0x00fbu),
+                             0x5410u);
+    const unsigned s1 = sm & 0x01010101u;
+    unsigned zh[4], zl[4], d8[4];
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      const double y = mul ? fabs(v[4 * q + i]) * inv : fabs(scalbn(v[4 * q + i], -e));
+      const double z = __dadd_rz(y, 1.0);
+      zh[i] = (unsigned)__double2hiint(z);
+      zl[i] = (unsigned)__double2loint(z);
+      if constexpr (S == 8) {
+        const double tail = y - (z - 1.0);  // exact: the bits of |y| below 2^-52
+        d8[i] = ((zl[i] & 7u) << 4) | (unsigned)__double2int_rz(tail * 72057594037927936.0);
+      }
+    }
+#pragma unroll
+    for (int t = 1; t <= S; ++t) {
+      unsigned x[4];
+#pragma unroll
+      for (int i = 0; i < 4; ++i) {
+        // fraction bits 7t-6 .. 7t of z sit at mantissa bits 58-7t .. 52-7t
+        if (t == 1) x[i] = zh[i] >> 13;
+        else if (t == 2) x[i] = zh[i] >> 6;
+        else if (t == 3) x[i] = __funnelshift_r(zl[i], zh[i], 31);
+        else if (t == 4) x[i] = zl[i];  // already byte-aligned: byte 3
+        else if (t == 5) x[i] = zl[i] >> 17;
+        else if (t == 6) x[i] = zl[i] >> 10;
+        else if (t == 7) x[i] = zl[i] >> 3;
+        else x[i] = d8[i];
+      }
+      const unsigned sel = t == 4 ? 0x73u : 0x40u;  // byte 0 (or 3) of the first and second word
+      const unsigned pk = prmt(prmt(x[0], x[1], sel), prmt(x[2], x[3], sel), 0x5410u);
+      w[t - 1][q] = (((pk ^ sm) & 0x7f7f7f7fu) + s1) ^ (sm & 0x80808080u);
+    }
+  }
+#pragma unroll
+  for (int t = 0; t < S; ++t)
+    *reinterpret_cast<int2*>(out + base + t * slab) = make_int2((int)w[t][0], (int)w[t][1]);
+}
+
+// Items of 32 rows of one block; a 256-thread CTA walks a contiguous range of them.  Lane = row;
+// warp w takes the 8-wide k-chunks w, w+8, ... of the row (a warp's load of one k is 32
+// consecutive rows of a column-major block).  An item with K <= 64 (every row one chunk per
+// warp at most) is copied into shared memory (8-byte cp.async, zero-filled past the block)
+// while the CTA slices the previous one: two buffers, one item ahead.  Rows with K > 64 read
+// their values from global memory twice (maximum, then slices).  The row maximum is reduced
+// over the eight warps in shared memory and gives the row's exponent e (rows padded up to the
+// tile height R get 0); the slices are stored in tile order:
 //   out[((tile * ksteps + ks) * S + t) * R * 32 + slab_offset(row % R, k)].
 // Rows past the block and k past K are zero.  With pscale set (B columns), the row's scale 2^e
-// is also written as a double (0 when e is outside [elo, ehi]).  Rows with more than four
-// chunks (K > 64) read their values a second time for the slicing.
-constexpr int kSliceWarps = 4;
-__global__ void __launch_bounds__(kSliceWarps * 32, 5) k_slice(
-    const double* __restrict__ src, const long long* __restrict__ src_off, const int* __restrict__ dims, int order,
-    ModeMap fm, ModeMap km, const long long* __restrict__ out_off, const long long* __restrict__ exp_off,
-    signed char* __restrict__ out, short* __restrict__ expo, double* __restrict__ pscale, int elo, int ehi,
-    double scale, int S, int R, const long long* __restrict__ istart, long long nblocks, long long nitems,
-    int* __restrict__ flags) {
+// is also written as a double (0 when e is outside [elo, ehi]).
+constexpr int kSliceWarps = 8, kSliceHoldK = 64, kSliceCtas = 4;  // CTAs per SM
+template <int S>
+__global__ void __launch_bounds__(kSliceWarps * 32, kSliceCtas) k_slice(const __grid_constant__ SliceArgs g) {
+  __shared__ __align__(16) double buf[2][kSliceHoldK][32];
   __shared__ double wmax[kSliceWarps][32];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  for (long long it = blockIdx.x; it < nitems; it += gridDim.x) {
-    // the block holding item it: the last block whose first item is <= it
-    long long lo = 0, hi = nblocks;
-    while (hi - lo > 1) {
-      const long long mid = (lo + hi) >> 1;
-      if (istart[mid] <= it) lo = mid; else hi = mid;
-    }
-    const long long b = lo;
-    const int r = (int)(it - istart[b]) * 32 + lane;
-    const int* d = dims + b * order;
+  const long long nitems = g.op[0].nitems + g.op[1].nitems;
+  const long long per = (nitems + gridDim.x - 1) / gridDim.x;
+  const long long i0 = blockIdx.x * per, i1 = min(nitems, i0 + per);
+  if (i0 >= i1) return;
+
+  // copies of item L into buffer bi (nothing for an item with K > 64)
+  auto prefetch = [&](const SliceLoc& L, int bi) {
+    if (L.K > kSliceHoldK) return;
+    const SliceOperand& o = g.op[L.opb];
+    const int* d = o.dims + L.b * o.order;
     int st[kMaxOrder];
-    block_strides(d, order, st);
-    int m = 1, K = 1;
-    for (int t = 0; t < fm.n; ++t) m *= d[fm.x[t]];
-    for (int t = 0; t < km.n; ++t) K *= d[km.x[t]];
-    const int Kp = (K + kSplitK - 1) / kSplitK * kSplitK;
-    const int ksteps = Kp / kSplitK, nchunks = Kp / 16;
-    auto offset = [&](const ModeMap& mm, int idx) {
-      int off = 0;
-      for (int t = 0; t < mm.n; ++t) {
-        const int e = d[mm.x[t]];
-        off += (idx % e) * st[mm.x[t]];
-        idx /= e;
-      }
-      return off;
-    };
-    // contracted offsets: one contracted mode (the common case) is a plain stride
-    const bool k1 = km.n == 1;
-    const int kst = k1 ? st[km.x[0]] : 0;
-    auto koff = [&](int k) { return k1 ? k * kst : offset(km, k); };
-    const double* s = src + src_off[b];
-    const bool live = r < m;
-    const int fr = live ? offset(fm, r) : 0;
-    auto load_chunk = [&](int c, double (&v)[16]) {
+    block_strides(d, o.order, st);
+    const bool live = L.r < L.m;
+    const double* src = o.src + o.src_off[L.b];
+    const double* row = live ? src + mode_offset(d, st, o.fm, L.r) : src;
+    const int Kp = (L.K + kSplitK - 1) / kSplitK * kSplitK;
+    if (o.km.n == 1) {
+      const int kst = st[o.km.x[0]];
 #pragma unroll
-      for (int j = 0; j < 16; ++j) {
-        const int k = c * 16 + j;
-        v[j] = (live && k < K) ? __dmul_rn(s[fr + koff(k)], scale) : 0.0;
+      for (int i = 0; i < kSliceHoldK / kSliceWarps; ++i) {
+        const int k = warp + i * kSliceWarps;
+        const bool in = live && k < L.K;
+        if (k < Kp) cp_async8(&buf[bi][k][lane], in ? row + k * kst : src, in ? 8 : 0);
+      }
+    } else {
+      for (int k = warp; k < Kp; k += kSliceWarps) {
+        const bool in = live && k < L.K;
+        cp_async8(&buf[bi][k][lane], in ? row + mode_offset(d, st, o.km, k) : src, in ? 8 : 0);
+      }
+    }
+  };
+
+  SliceLoc none;
+  none.opb = -1;
+  SliceLoc cur = slice_locate(g, i0, none, lane);
+  prefetch(cur, 0);
+  cp_async_commit8();
+  for (long long item = i0; item < i1; ++item) {
+    const int bi = (int)((item - i0) & 1);
+    SliceLoc nxt = cur;
+    if (item + 1 < i1) {
+      nxt = slice_locate(g, item + 1, cur, lane);
+      prefetch(nxt, bi ^ 1);  // that buffer was last read by the previous item (barrier below)
+    }
+    cp_async_commit8();
+    cp_async_wait8<1>();  // this thread's copies of the current item have landed
+    __syncthreads();      // and every thread's
+
+    const SliceOperand& o = g.op[cur.opb];
+    const int* d = o.dims + cur.b * o.order;
+    const int R = o.R, K = cur.K, r = cur.r;
+    const int Kp = (K + kSplitK - 1) / kSplitK * kSplitK;
+    const int ksteps = Kp / kSplitK, nchunks = Kp / 8;
+    const bool hold = K <= kSliceHoldK, live = r < cur.m;
+    const double scale = o.scale;
+    // the direct path's addressing (K > 64)
+    int st[kMaxOrder];
+    const bool k1 = o.km.n == 1;
+    int kst = 0;
+    const double* row = nullptr;
+    if (!hold) {
+      block_strides(d, o.order, st);
+      kst = k1 ? st[o.km.x[0]] : 0;
+      row = o.src + o.src_off[cur.b] + (live ? mode_offset(d, st, o.fm, r) : 0);
+    }
+    auto load_chunk = [&](int c, double (&v)[8]) {
+#pragma unroll
+      for (int j = 0; j < 8; ++j) {
+        const int k = c * 8 + j;
+        const bool in = live && k < K;
+        if (hold) v[j] = in ? __dmul_rn(buf[bi][k][lane], scale) : 0.0;
+        else v[j] = in ? __dmul_rn(row[k1 ? k * kst : mode_offset(d, st, o.km, k)], scale) : 0.0;
       }
     };
-    // pass over this warp's chunks; when the row has at most kSliceWarps chunks (K <= 64) each
-    // warp has at most one, and it stays in registers for the slicing
-    const bool hold = nchunks <= kSliceWarps;
-    double v[16];
+    double v[8];
     double mx = 0.0;
     bool finite = true;
     for (int c = warp; c < nchunks; c += kSliceWarps) {
       load_chunk(c, v);
 #pragma unroll
-      for (int j = 0; j < 16; ++j) {
+      for (int j = 0; j < 8; ++j) {
         finite = finite && isfinite(v[j]);
         mx = fmax(mx, fabs(v[j]));
       }
     }
-    if (!finite) atomicExch(&flags[kFlagNonFinite], 1);
+    if (!finite) atomicExch(&g.flags[kFlagNonFinite], 1);
     wmax[warp][lane] = mx;
     __syncthreads();
-    mx = fmax(fmax(wmax[0][lane], wmax[1][lane]), fmax(wmax[2][lane], wmax[3][lane]));
-    __syncthreads();  // wmax is rewritten by the next item
+#pragma unroll
+    for (int w = 0; w < kSliceWarps; ++w) mx = fmax(mx, wmax[w][lane]);
     int e = 0;
     if (mx > 0.0) frexp(mx, &e);
+    const long long eo = o.exp_off[cur.b];
     if (warp == 0) {
-      expo[exp_off[b] + r] = (short)e;
-      const bool in_range = e >= elo && e <= ehi;
-      if (!in_range) atomicExch(&flags[kFlagGeneralExp], 1);
-      if (pscale) pscale[exp_off[b] + r] = in_range ? ldexp(1.0, e) : 0.0;
+      o.expo[eo + r] = (short)e;
+      const bool in_range = e >= o.elo && e <= o.ehi;
+      if (!in_range) atomicExch(&g.flags[kFlagGeneralExp], 1);
+      if (o.pscale) o.pscale[eo + r] = in_range ? ldexp(1.0, e) : 0.0;
     }
-    // slices of every chunk of this warp: 16 k at a time, the S slices packed four bytes to a
-    // register and stored as one 16-byte word each.  v * 2^-e is exact when 2^-e is a normal
-    // double and the product is normal; a product below 2^-1022 has only zero slices either
-    // way.  Other exponents scale with scalbn.
-    const bool mul = e >= -1022 && e <= 1022;
-    const double inv = mul ? __longlong_as_double((long long)(1023 - e) << 52) : 0.0;
-    signed char* o = out + out_off[b] + (long long)(r / R) * ksteps * S * R * kSplitK;
+    signed char* out = o.out + o.out_off[cur.b] + (long long)(r / R) * ksteps * S * R * kSplitK;
+    const long long slab = (long long)R * kSplitK;
     for (int c = warp; c < nchunks; c += kSliceWarps) {
       if (!hold) load_chunk(c, v);
-#pragma unroll
-      for (int j = 0; j < 16; ++j) v[j] = mul ? v[j] * inv : scalbn(v[j], -e);
-      // slice t of the 16 values from their running remainders, stored as soon as it is packed
-      const long long base = (long long)(c / 2) * S * R * kSplitK + slab_offset(r % R, (c & 1) * 16);
-      for (int t = 0; t < S; ++t) {
-        unsigned w[4] = {0u, 0u, 0u, 0u};
-#pragma unroll
-        for (int j = 0; j < 16; ++j) {
-          const double y = v[j] * 128.0;
-          const double tr = trunc(y);
-          // the integer tr (|tr| <= 127) in the low word of 1.5 * 2^52 + tr, exactly
-          const unsigned bits = (unsigned)__double2loint(tr + 6755399441055744.0);
-          w[j >> 2] |= (bits & 0xffu) << ((j & 3) * 8);
-          v[j] = y - tr;
-        }
-        *reinterpret_cast<int4*>(o + base + (long long)t * R * kSplitK) =
-            make_int4((int)w[0], (int)w[1], (int)w[2], (int)w[3]);
-      }
+      slice_chunk<S>(v, e, out, (long long)(c / 4) * S * slab + slab_offset(r % R, (c & 3) * 8), slab);
     }
+    __syncthreads();  // wmax and this item's buffer are rewritten from the next item on
+    cur = nxt;
   }
+  cp_async_wait8<0>();
 }
+using SliceKernel = void (*)(SliceArgs);
+static const SliceKernel kSliceKernels[kMaxSlices] = {k_slice<1>, k_slice<2>, k_slice<3>, k_slice<4>,
+                                                      k_slice<5>, k_slice<6>, k_slice<7>, k_slice<8>};
 
 // ------------------------------------------------------------------ tcgen05 helpers
 __device__ __forceinline__ unsigned smem_u32(const void* p) { return static_cast<unsigned>(__cvta_generic_to_shared(p)); }
@@ -332,18 +504,20 @@ struct SplitPair {
 };
 
 // Element offsets, within their C block, of every row and every column of every C block
-// (rows of block c at rowtab[rowbase[c] ..], columns at coltab[colbase[c] ..]).
+// (rows of block c at rowtab[rowbase[c] ..], columns at coltab[colbase[c] ..]).  One warp per
+// C block.
 __global__ void k_split_offsets(const int* __restrict__ dimsC, long long nc, TileMaps mp,
                                 const long long* __restrict__ rowbase, const long long* __restrict__ colbase,
                                 int* __restrict__ rowtab, int* __restrict__ coltab) {
-  for (long long c = blockIdx.x; c < nc; c += gridDim.x) {
+  const int lane = threadIdx.x & 31, wpb = blockDim.x >> 5;
+  for (long long c = (long long)blockIdx.x * wpb + (threadIdx.x >> 5); c < nc; c += (long long)gridDim.x * wpb) {
     const int* cd = dimsC + c * mp.oC;
     int st[kMaxOrder];
     block_strides(cd, mp.oC, st);
     int m = 1, n = 1;
     for (int q = 0; q < mp.row.n; ++q) m *= cd[mp.row.y[q]];
     for (int q = 0; q < mp.col.n; ++q) n *= cd[mp.col.y[q]];
-    for (int r = threadIdx.x; r < m; r += blockDim.x) {
+    for (int r = lane; r < m; r += 32) {
       int x = r, off = 0;
       for (int q = 0; q < mp.row.n; ++q) {
         const int e = cd[mp.row.y[q]];
@@ -352,7 +526,7 @@ __global__ void k_split_offsets(const int* __restrict__ dimsC, long long nc, Til
       }
       rowtab[rowbase[c] + r] = off;
     }
-    for (int j = threadIdx.x; j < n; j += blockDim.x) {
+    for (int j = lane; j < n; j += 32) {
       int x = j, off = 0;
       for (int q = 0; q < mp.col.n; ++q) {
         const int e = cd[mp.col.y[q]];
@@ -1091,7 +1265,7 @@ void split_records(sht_plan* p, cudaStream_t s) {
   SHT_CUDA(cudaMemsetAsync(p->sp_rowtab.ptr, 0, (rtot + kSplitM) * 4, s));
   SHT_CUDA(cudaMemsetAsync(p->sp_coltab.ptr, 0, (ctot + kSplitN) * 4, s));
   if (nc > 0)
-    k_split_offsets<<<(int)std::min<long long>(nc, (long long)p->ctx->num_sms * 8), 128, 0, s>>>(
+    k_split_offsets<<<(int)std::min<long long>((nc + 7) / 8, (long long)p->ctx->num_sms * 8), 256, 0, s>>>(
         C->d_dims.as<int>(), nc, p->tmaps, drb.as<long long>(), dcb.as<long long>(), p->sp_rowtab.as<int>(),
         p->sp_coltab.as<int>());
   trace("split: C offset tables", s);
@@ -1175,20 +1349,50 @@ void split_slice(sht_plan* p, double alpha, cudaStream_t s) {
   std::memcpy(&ab, &alpha, 8);
   // the execute's flag words start clear (the slicer sets them)
   SHT_CUDA(cudaMemsetAsync(p->sp_err, 0, 8, s));
-  if (ab != 0) {
-    const long long cap = (long long)p->ctx->num_sms * 32;
-    if (p->sp_naitems)
-      k_slice<<<(int)std::min(p->sp_naitems, cap), kSliceWarps * 32, 0, s>>>(
-          p->A->d_data.as<double>(), p->A->d_offsets.as<long long>(), p->A->d_dims.as<int>(), p->A->order,
-          modes_of(p->maps.rowA), modes_of(p->maps.colA), p->sp_aoff, p->sp_aeoff,
-          p->sp_a.as<signed char>(), p->sp_ae.as<short>(), nullptr, kExpLoA, kExpHiA, alpha, S, kSplitM,
-          p->sp_aistart, p->A->nblocks, p->sp_naitems, p->sp_err);
-    if (p->sp_nbitems)
-      k_slice<<<(int)std::min(p->sp_nbitems, cap), kSliceWarps * 32, 0, s>>>(
-          p->B->d_data.as<double>(), p->B->d_offsets.as<long long>(), p->B->d_dims.as<int>(), p->B->order,
-          modes_of(p->maps.colB), modes_of(p->maps.rowB), p->sp_boff, p->sp_beoff,
-          p->sp_b.as<signed char>(), p->sp_be.as<short>(), p->sp_bsc.as<double>(), kExpLoB, kExpHiB, 1.0, S,
-          kSplitN, p->sp_bistart, p->B->nblocks, p->sp_nbitems, p->sp_err);
+  if (ab != 0 && p->sp_naitems + p->sp_nbitems > 0) {
+    SliceArgs g{};
+    SliceOperand& a = g.op[0];
+    a.src = p->A->d_data.as<double>();
+    a.src_off = p->A->d_offsets.as<long long>();
+    a.dims = p->A->d_dims.as<int>();
+    a.out_off = p->sp_aoff;
+    a.exp_off = p->sp_aeoff;
+    a.istart = p->sp_aistart;
+    a.out = p->sp_a.as<signed char>();
+    a.expo = p->sp_ae.as<short>();
+    a.pscale = nullptr;
+    a.scale = alpha;
+    a.nblocks = p->A->nblocks;
+    a.nitems = p->sp_naitems;
+    a.fm = modes_of(p->maps.rowA);
+    a.km = modes_of(p->maps.colA);
+    a.order = p->A->order;
+    a.R = kSplitM;
+    a.elo = kExpLoA;
+    a.ehi = kExpHiA;
+    SliceOperand& bo = g.op[1];
+    bo.src = p->B->d_data.as<double>();
+    bo.src_off = p->B->d_offsets.as<long long>();
+    bo.dims = p->B->d_dims.as<int>();
+    bo.out_off = p->sp_boff;
+    bo.exp_off = p->sp_beoff;
+    bo.istart = p->sp_bistart;
+    bo.out = p->sp_b.as<signed char>();
+    bo.expo = p->sp_be.as<short>();
+    bo.pscale = p->sp_bsc.as<double>();
+    bo.scale = 1.0;
+    bo.nblocks = p->B->nblocks;
+    bo.nitems = p->sp_nbitems;
+    bo.fm = modes_of(p->maps.colB);
+    bo.km = modes_of(p->maps.rowB);
+    bo.order = p->B->order;
+    bo.R = kSplitN;
+    bo.elo = kExpLoB;
+    bo.ehi = kExpHiB;
+    g.flags = p->sp_err;
+    // one wave of resident CTAs, each over a contiguous range of items
+    const long long cap = (long long)p->ctx->num_sms * kSliceCtas;
+    kSliceKernels[S - 1]<<<(int)std::min(p->sp_naitems + p->sp_nbitems, cap), kSliceWarps * 32, 0, s>>>(g);
     SHT_CUDA(cudaGetLastError());
   }
 }
