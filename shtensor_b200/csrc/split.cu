@@ -275,7 +275,7 @@ __global__ void __launch_bounds__(kSliceWarps * 32, kSliceCtas) k_slice(const __
 
   // copies of item L into buffer bi (nothing for an item with K > 64)
   auto prefetch = [&](const SliceLoc& L, int bi) {
-    if (L.K > kSliceHoldK) return;
+    if (L.K > kSliceHoldK || L.r - lane >= L.m) return;  // read directly, or rows all past the block
     const SliceOperand& o = g.op[L.opb];
     const int* d = o.dims + L.b * o.order;
     int st[kMaxOrder];
@@ -322,6 +322,9 @@ __global__ void __launch_bounds__(kSliceWarps * 32, kSliceCtas) k_slice(const __
     const int Kp = (K + kSplitK - 1) / kSplitK * kSplitK;
     const int ksteps = Kp / kSplitK, nchunks = Kp / 8;
     const bool hold = K <= kSliceHoldK, live = r < cur.m;
+    // chunks holding a value: none when the item's rows all lie past the block (padding up to
+    // the tile height), and none past K; the others are stored as zero slices
+    const int nvalued = r - lane >= cur.m ? 0 : (K + 7) / 8;
     const double scale = o.scale;
     // the direct path's addressing (K > 64)
     int st[kMaxOrder];
@@ -345,7 +348,7 @@ __global__ void __launch_bounds__(kSliceWarps * 32, kSliceCtas) k_slice(const __
     double v[8];
     double mx = 0.0;
     bool finite = true;
-    for (int c = warp; c < nchunks; c += kSliceWarps) {
+    for (int c = warp; c < nvalued; c += kSliceWarps) {
       load_chunk(c, v);
 #pragma unroll
       for (int j = 0; j < 8; ++j) {
@@ -370,8 +373,14 @@ __global__ void __launch_bounds__(kSliceWarps * 32, kSliceCtas) k_slice(const __
     signed char* out = o.out + o.out_off[cur.b] + (long long)(r / R) * ksteps * S * R * kSplitK;
     const long long slab = (long long)R * kSplitK;
     for (int c = warp; c < nchunks; c += kSliceWarps) {
-      if (!hold) load_chunk(c, v);
-      slice_chunk<S>(v, e, out, (long long)(c / 4) * S * slab + slab_offset(r % R, (c & 3) * 8), slab);
+      const long long base = (long long)(c / 4) * S * slab + slab_offset(r % R, (c & 3) * 8);
+      if (c < nvalued) {
+        if (!hold) load_chunk(c, v);
+        slice_chunk<S>(v, e, out, base, slab);
+      } else {
+#pragma unroll
+        for (int t = 0; t < S; ++t) *reinterpret_cast<int2*>(out + base + t * slab) = make_int2(0, 0);
+      }
     }
     __syncthreads();  // wmax and this item's buffer are rewritten from the next item on
     cur = nxt;
