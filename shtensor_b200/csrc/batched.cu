@@ -333,7 +333,7 @@ __global__ void k_collect(ScalarSrc src, long long* __restrict__ out) {
 }
 
 void device_work_list(sht_plan* p, int fixed_tm, int fixed_tn, bool per_class, cudaStream_t s, const DevSum* extra,
-                      long long* extra_out, int nextra) {
+                      long long* extra_out, int nextra, const unsigned long long* order_key, int order_bits) {
   if (nextra > 3) fail(SHT_ERR_INVALID, "work list: at most three extra scalars");
   DevicePool* pool = p->ctx->pool.get();
   const long long nc = p->ncblk;
@@ -365,14 +365,24 @@ void device_work_list(sht_plan* p, int fixed_tm, int fixed_tn, bool per_class, c
       table.as<unsigned char>(), per_class ? 0 : fixed_tm, fixed_tn, ss, shape.as<int>(), tiles.as<long long>(),
       ttiles.as<long long>(), key.as<unsigned long long>(), idx.as<int>());
   SHT_CUDA(cudaGetLastError());
+  // a caller's order (ascending keys, untouched blocks keyed last) replaces the cost order
+  auto sort_blocks = [&](void* tmp_ptr, size_t& bytes) {
+    if (order_key)
+      cub::DeviceRadixSort::SortPairs(tmp_ptr, bytes, key.as<unsigned long long>(), key2.as<unsigned long long>(),
+                                      idx.as<int>(), idx2.as<int>(), (int)nc, 0, order_bits, s);
+    else
+      cub::DeviceRadixSort::SortPairsDescending(tmp_ptr, bytes, key.as<unsigned long long>(),
+                                                key2.as<unsigned long long>(), idx.as<int>(), idx2.as<int>(), (int)nc, 0,
+                                                16, s);
+  };
+  if (order_key)
+    SHT_CUDA(cudaMemcpyAsync(key.ptr, order_key, nc * 8, cudaMemcpyDeviceToDevice, s));
   size_t tb = 0, tb2 = 0, tb3 = 0;
-  cub::DeviceRadixSort::SortPairsDescending(nullptr, tb, key.as<unsigned long long>(), key2.as<unsigned long long>(),
-                                            idx.as<int>(), idx2.as<int>(), (int)nc, 0, 16, s);
+  sort_blocks(nullptr, tb);
   cub::DeviceScan::ExclusiveSum(nullptr, tb2, tsorted.as<long long>(), off.as<long long>(), (int)nc, s);
   cub::DeviceReduce::Sum(nullptr, tb3, ttiles.as<long long>(), sums.as<long long>(), (int)nc, s);
   PoolBuf tmp(pool, std::max(tb, std::max(tb2, tb3)), s);
-  cub::DeviceRadixSort::SortPairsDescending(tmp.ptr, tb, key.as<unsigned long long>(), key2.as<unsigned long long>(),
-                                            idx.as<int>(), idx2.as<int>(), (int)nc, 0, 16, s);
+  sort_blocks(tmp.ptr, tb);
   k_gather_tiles<<<grid_for(nc, 256), 256, 0, s>>>(idx2.as<int>(), tiles.as<long long>(), nc, tsorted.as<long long>());
   cub::DeviceScan::ExclusiveSum(tmp.ptr, tb2, tsorted.as<long long>(), off.as<long long>(), (int)nc, s);
   cub::DeviceReduce::Sum(tmp.ptr, tb3, ttiles.as<long long>(), sums.as<long long>(), (int)nc, s);

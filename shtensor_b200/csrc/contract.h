@@ -89,8 +89,11 @@ struct DevSum {
   const long long* b;
 };
 // extra (up to three device scalars) are read back with the list's own counts into extra_out.
+// order_key (per C block, ascending, order_bits wide; blocks without pairs must key last)
+// replaces the cost order when given.
 void device_work_list(sht_plan* p, int fixed_tm, int fixed_tn, bool per_class, cudaStream_t s,
-                      const DevSum* extra = nullptr, long long* extra_out = nullptr, int nextra = 0);
+                      const DevSum* extra = nullptr, long long* extra_out = nullptr, int nextra = 0,
+                      const unsigned long long* order_key = nullptr, int order_bits = 0);
 void plan_execute(sht_plan* p, double alpha, double beta, cudaStream_t s);
 void batched_prepare(sht_plan* p, cudaStream_t s);
 // the persistent kernel alone, with the operands already in matrix form (matform_execute)

@@ -31,8 +31,12 @@
 //               pair's groups while the tensor cores already work on the next pair (second
 //               TMEM set), accumulate in registers, store the tile at the end;
 //   warp 10     record warp: resolves each pair's copy sources and exponent rows into a
-//               shared ring that the producer and the MMA issuer read;
-//   warp 11     idle (it only lifts the register allowance to 168 per thread).
+//               shared ring that the producer, the MMA issuer and the slot warp read;
+//   warp 11     slot warp: loads each tile's record and row / column offsets, and each
+//               pair's row exponents, column exponents and column scales, into the tile and
+//               exponent rings with ordinary loads and stores.  The bulk copies of one SM
+//               run one after another, each taking hundreds of cycles however small, so
+//               only the operand slabs (two large copies per k-step) go through them.
 // Per-tile and per-pair records are built at plan time so that each role reads one record
 // per tile and per pair.  Every wait is bounded: a role that gives up raises a CTA-wide abort
 // flag and the error word (SHT_ERR_TIMEOUT); the others leave their waits on the flag, the
@@ -70,7 +74,8 @@ constexpr int kEpiCols = kSplitN / (kEpiWarps / 4);  // tile columns per epilogu
 constexpr int kTileSlots = 4, kExpSlots = 4;    // depth of the tile-record and exponent rings
 constexpr int kRecSlots = 16;                   // depth of the record ring (power of two)
 constexpr int kRecWarp = 2 + kEpiWarps;         // the record warp, after the epilogue warps
-// 12 warps: producer, MMA issuer, 8 epilogue warps, record warp, one idle warp.  Twelve warps
+constexpr int kSlotWarp = kRecWarp + 1;         // the slot warp, last
+// 12 warps: producer, MMA issuer, 8 epilogue warps, record warp, slot warp.  Twelve warps
 // put three on each SM sub-partition, whose 16K registers then allow 168 per thread (eleven
 // would allow only 160 per thread under the launch bound's rounding).
 constexpr int kSplitThreads = 64 + kEpiWarps * 32 + 64;
@@ -156,6 +161,14 @@ __device__ __forceinline__ int mode_offset(const int* d, const int* st, const Mo
     idx /= e;
   }
   return off;
+}
+
+// True when the modes mm are consecutive and ascending (x[t+1] = x[t] + 1): the column-major
+// strides then compose, and combined index idx lies at idx * st[x[0]] in every block.
+__device__ __forceinline__ bool linear_modes(const ModeMap& mm) {
+  bool lin = true;
+  for (int t = 1; t < mm.n; ++t) lin = lin && mm.x[t] == mm.x[t - 1] + 1;
+  return lin;
 }
 
 // Where one slicer item lies: its operand, its block (and the block's item range), the block's
@@ -284,7 +297,7 @@ __global__ void __launch_bounds__(kSliceWarps * 32, kSliceCtas) k_slice(const __
     const double* src = o.src + o.src_off[L.b];
     const double* row = live ? src + mode_offset(d, st, o.fm, L.r) : src;
     const int Kp = (L.K + kSplitK - 1) / kSplitK * kSplitK;
-    if (o.km.n == 1) {
+    if (linear_modes(o.km)) {
       const int kst = st[o.km.x[0]];
 #pragma unroll
       for (int i = 0; i < kSliceHoldK / kSliceWarps; ++i) {
@@ -328,7 +341,7 @@ __global__ void __launch_bounds__(kSliceWarps * 32, kSliceCtas) k_slice(const __
     const double scale = o.scale;
     // the direct path's addressing (K > 64)
     int st[kMaxOrder];
-    const bool k1 = o.km.n == 1;
+    const bool k1 = linear_modes(o.km);  // k at k * kst (no per-element index division)
     int kst = 0;
     const double* row = nullptr;
     if (!hold) {
@@ -348,8 +361,20 @@ __global__ void __launch_bounds__(kSliceWarps * 32, kSliceCtas) k_slice(const __
     double v[8];
     double mx = 0.0;
     bool finite = true;
-    for (int c = warp; c < nvalued; c += kSliceWarps) {
-      load_chunk(c, v);
+    int c0 = warp;
+    // two chunks per step: sixteen loads in flight per thread on the direct path
+    for (; c0 + kSliceWarps < nvalued; c0 += 2 * kSliceWarps) {
+      double v2[8];
+      load_chunk(c0, v);
+      load_chunk(c0 + kSliceWarps, v2);
+#pragma unroll
+      for (int j = 0; j < 8; ++j) {
+        finite = finite && isfinite(v[j]) && isfinite(v2[j]);
+        mx = fmax(mx, fmax(fabs(v[j]), fabs(v2[j])));
+      }
+    }
+    if (c0 < nvalued) {
+      load_chunk(c0, v);
 #pragma unroll
       for (int j = 0; j < 8; ++j) {
         finite = finite && isfinite(v[j]);
@@ -445,9 +470,6 @@ __device__ __forceinline__ void tmem_ld8(unsigned taddr, unsigned* v) {
                : "r"(taddr)
                : "memory");
 }
-// Orders this thread's generic-proxy shared-memory accesses before later async-proxy ones
-// (bulk copies into a buffer it has read).
-__device__ __forceinline__ void fence_proxy_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
 __device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
 __device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
 __device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
@@ -479,6 +501,23 @@ __device__ __forceinline__ void bulk_g2s(void* smem, const void* gmem, unsigned 
                    smem_u32(smem)),
                "l"(gmem), "r"(bytes), "r"(smem_u32(mbar))
                : "memory");
+}
+
+// L2 policy that keeps lines resident (evict last): the operand slices, read by many tiles
+__device__ __forceinline__ unsigned long long l2_keep_policy() {
+  unsigned long long pol;
+  asm volatile("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(pol));
+  return pol;
+}
+
+// bulk_g2s with an L2 cache policy for the source lines
+__device__ __forceinline__ void bulk_g2s_hint(void* smem, const void* gmem, unsigned bytes, void* mbar,
+                                              unsigned long long pol) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes.L2::cache_hint [%0], [%1], %2, [%3], %4;" ::"r"(
+          smem_u32(smem)),
+      "l"(gmem), "r"(bytes), "r"(smem_u32(mbar)), "l"(pol)
+      : "memory");
 }
 
 // int64 -> double for |x| < 2^51 with one integer add and one FP64 add: the bits of
@@ -556,6 +595,23 @@ __global__ void k_round4(const int* __restrict__ cm, const int* __restrict__ cn,
   }
 }
 
+// Work order of a split plan with many C blocks: by the block coordinates of C's row modes (the
+// modes A contributes), so that tiles reading the same A row slabs run close together in time
+// and find them in L2; blocks without pairs key last (flag bit `rbits`).
+__global__ void k_split_order_keys(const long long* __restrict__ ids, long long nc, TensorMeta mC, ModeMap row,
+                                   const int* __restrict__ pstart, int rbits, unsigned long long* __restrict__ key) {
+  for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < nc; c += (long long)gridDim.x * blockDim.x) {
+    const long long id = ids[c];
+    unsigned long long k = 0, mul = 1;
+    for (int t = 0; t < row.n; ++t) {
+      const int y = row.y[t];
+      k += (unsigned long long)((id / mC.gstride[y]) % mC.nblk[y]) * mul;
+      mul *= (unsigned long long)mC.nblk[y];
+    }
+    key[c] = k | (pstart[c + 1] > pstart[c] ? 0ull : 1ull << rbits);
+  }
+}
+
 __global__ void k_split_items(const int4* __restrict__ work, int nwork, const int* __restrict__ pstart,
                               const long long* __restrict__ offC, const int* __restrict__ dimsC, TileMaps mp,
                               const long long* __restrict__ rowbase, const long long* __restrict__ colbase,
@@ -566,11 +622,12 @@ __global__ void k_split_items(const int4* __restrict__ work, int nwork, const in
     int m = 1, n = 1;
     for (int q = 0; q < mp.row.n; ++q) m *= cd[mp.row.y[q]];
     for (int q = 0; q < mp.col.n; ++q) n *= cd[mp.col.y[q]];
-    const int ntr = (m + kSplitM - 1) / kSplitM;
+    const int ntc = (n + kSplitN - 1) / kSplitN;
     SplitItem t;
     t.cbase = offC[w.x];
-    t.r0 = (w.y % ntr) * kSplitM;
-    t.c0 = (w.y / ntr) * kSplitN;
+    // column tiles of one row tile one after another: they read the same A slabs
+    t.r0 = (w.y / ntc) * kSplitM;
+    t.c0 = (w.y % ntc) * kSplitN;
     t.rtab = (int)(rowbase[w.x] + t.r0);
     t.ctab = (int)(colbase[w.x] + t.c0);
     t.pb = pstart[w.x];
@@ -626,11 +683,11 @@ struct SplitArgs {
   long long drain_limit;   // polls of the waits for work already issued (copies, MMAs)
 };
 
-// Per tile, the producer also copies the tile's record and its row / column offsets into a
-// ring of tile slots, and per pair the A row exponents, the B column exponents and the B
-// column scales into a ring of exponent slots, so the epilogue reads nothing from global
-// memory but the C values it scales by beta.
-// One record of the producer's and the MMA issuer's work stream: one pair of one tile (or a
+// Per tile, the slot warp loads the tile's record and its row / column offsets into a ring of
+// tile slots, and per pair the A row exponents, the B column exponents and the B column
+// scales into a ring of exponent slots, so the epilogue reads nothing from global memory but
+// the C values it scales by beta.
+// One record of the producer's, the MMA issuer's and the slot warp's work stream: one pair of one tile (or a
 // tile without pairs), its copy sources resolved by the record warp.
 struct SplitRec {
   const signed char* a_src;  // A slabs of the pair's k-steps for the tile's rows
@@ -660,7 +717,7 @@ constexpr unsigned kTileSlotBytes = sizeof(SplitTileSlot);
 constexpr unsigned kExpSlotBytes = sizeof(SplitExpSlot);
 static_assert(sizeof(SplitItem) % 16 == 0 && kTileSlotBytes == 48 + 4 * (kSplitM + kSplitN) &&
                   kExpSlotBytes == 2 * (kSplitM + kSplitN) + 8 * kSplitN && offsetof(SplitExpSlot, sc) % 16 == 0,
-              "slot members are bulk-copy destinations at 16-byte offsets");
+              "slot members are filled by 16-byte stores at 16-byte offsets");
 
 template <int S>
 struct SplitSmem {
@@ -807,16 +864,16 @@ __global__ void __launch_bounds__(kSplitThreads, 1) k_split(const __grid_constan
       mbar_init(&sm.tempty[i], kEpiWarps);
     }
     for (int i = 0; i < kTileSlots; ++i) {
-      mbar_init(&sm.ifull[i], 1);
+      mbar_init(&sm.ifull[i], 32);  // every lane of the slot warp, after its own stores
       mbar_init(&sm.iempty[i], kEpiWarps);
     }
     for (int i = 0; i < kExpSlots; ++i) {
-      mbar_init(&sm.efull[i], 1);
+      mbar_init(&sm.efull[i], 32);
       mbar_init(&sm.eempty[i], kEpiWarps);
     }
     for (int i = 0; i < kRecSlots; ++i) {
       mbar_init(&sm.rfull[i], 1);
-      mbar_init(&sm.rempty[i], 2);  // the producer and the MMA issuer
+      mbar_init(&sm.rempty[i], 3);  // the producer, the MMA issuer and the slot warp
     }
     mbar_init(&sm.drain, 1);
     sm.abort = 0;
@@ -831,40 +888,27 @@ __global__ void __launch_bounds__(kSplitThreads, 1) k_split(const __grid_constan
   if (warp == 0) {
     // ---------------------------------------------------------------- producer
     if (lane == 0) {
-      long long n = 0, q = 0, ni = 0;
+      long long n = 0;
       int st = 0;         // stage of k-step n (n % kSplitStages) and its ring phase
       unsigned sph = 0;
       bool ok = true;
+      // the slices are read by every tile of their rows / columns: keep them in L2 against the
+      // stream of C stores (which the epilogue marks evict-first)
+      const unsigned long long keep = l2_keep_policy();
       for (long long r = 0; ok; ++r) {
         const int rs = (int)(r & (kRecSlots - 1));
         if (!split_wait(&sm.rfull[rs], (unsigned)((r / kRecSlots) & 1), abort, g)) { ok = false; break; }
         const SplitRec v = sm.rec[rs];
         mbar_arrive(&sm.rempty[rs]);
         if (v.kind & kRecEnd) break;
-        if (v.kind & kRecFirst) {
-          const int is = (int)(ni % kTileSlots);
-          if (!split_wait(&sm.iempty[is], (unsigned)(((ni / kTileSlots) & 1) ^ 1), abort, g)) { ok = false; break; }
-          ++ni;
-          mbar_expect_tx(&sm.ifull[is], kTileSlotBytes);
-          bulk_g2s(&sm.tile[is].rec, v.rec_src, sizeof(SplitItem), &sm.ifull[is]);
-          bulk_g2s(sm.tile[is].rowoff, v.rowtab_src, 4 * kSplitM, &sm.ifull[is]);
-          bulk_g2s(sm.tile[is].coloff, v.coltab_src, 4 * kSplitN, &sm.ifull[is]);
-        }
         if (v.ksteps == 0) continue;
-        const int es = (int)(q % kExpSlots);
-        if (!split_wait(&sm.eempty[es], (unsigned)(((q / kExpSlots) & 1) ^ 1), abort, g)) { ok = false; break; }
-        ++q;
-        mbar_expect_tx(&sm.efull[es], kExpSlotBytes);
-        bulk_g2s(sm.ex[es].ea, v.ae_src, 2 * kSplitM, &sm.efull[es]);
-        bulk_g2s(sm.ex[es].eb, v.be_src, 2 * kSplitN, &sm.efull[es]);
-        bulk_g2s(sm.ex[es].sc, v.bsc_src, 8 * kSplitN, &sm.efull[es]);
         const signed char* asrc = v.a_src;
         const signed char* bsrc = v.b_src;
         for (int ks = 0; ks < v.ksteps; ++ks, ++n) {
           if (!split_wait(&sm.empty[st], sph ^ 1u, abort, g)) { ok = false; break; }
           mbar_expect_tx(&sm.full[st], a_bytes + b_bytes);
-          bulk_g2s(sm.stage[st], asrc, a_bytes, &sm.full[st]);
-          bulk_g2s(sm.stage[st] + a_bytes, bsrc, b_bytes, &sm.full[st]);
+          bulk_g2s_hint(sm.stage[st], asrc, a_bytes, &sm.full[st], keep);
+          bulk_g2s_hint(sm.stage[st] + a_bytes, bsrc, b_bytes, &sm.full[st], keep);
           asrc += a_bytes;
           bsrc += b_bytes;
           if (++st == kSplitStages) {
@@ -880,8 +924,6 @@ __global__ void __launch_bounds__(kSplitThreads, 1) k_split(const __grid_constan
             split_settle(&bars[j % nbars], (unsigned)((j / nbars) & 1), g);
         };
         settle(sm.full, kSplitStages, n);
-        settle(sm.efull, kExpSlots, q);
-        settle(sm.ifull, kTileSlots, ni);
       }
     }
     __syncwarp();
@@ -997,6 +1039,56 @@ __global__ void __launch_bounds__(kSplitThreads, 1) k_split(const __grid_constan
       }
     }
     __syncwarp();
+  } else if (warp == kSlotWarp) {
+    // ---------------------------------------------------------------- slot warp
+    // Follows the record stream: per tile record it fills a tile slot (the tile's record and
+    // its row / column offsets), per pair an exponent slot (row exponents, column exponents,
+    // column scales), 16 bytes per lane.  The loads are issued before the wait for a free
+    // slot, which hides their latency while the warp runs ahead of the epilogue.  Every lane
+    // arrives on the slot's barrier after its own stores.
+    long long q = 0, ni = 0;
+    for (long long r = 0;; ++r) {
+      const int rs = (int)(r & (kRecSlots - 1));
+      if (!__all_sync(0xffffffffu, split_wait(&sm.rfull[rs], (unsigned)((r / kRecSlots) & 1), abort, g))) break;
+      const SplitRec v = sm.rec[rs];
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&sm.rempty[rs]);
+      if (v.kind & kRecEnd) break;
+      const bool first = (v.kind & kRecFirst) != 0, pair = v.ksteps > 0;
+      int4 t4 = make_int4(0, 0, 0, 0), ro = t4, co = t4, x0 = t4, x1 = t4;
+      if (first) {
+        if (lane < 3) t4 = reinterpret_cast<const int4*>(v.rec_src)[lane];       // 48-byte record
+        ro = reinterpret_cast<const int4*>(v.rowtab_src)[lane];                   // 128 row offsets
+        if (lane < 8) co = reinterpret_cast<const int4*>(v.coltab_src)[lane];     // 32 column offsets
+      }
+      if (pair) {
+        if (lane < 16) x0 = reinterpret_cast<const int4*>(v.ae_src)[lane];        // 128 row exponents
+        else if (lane < 20) x0 = reinterpret_cast<const int4*>(v.be_src)[lane - 16];  // 32 column exponents
+        if (lane < 16) x1 = reinterpret_cast<const int4*>(v.bsc_src)[lane];       // 32 column scales
+      }
+      if (first) {
+        const int is = (int)(ni % kTileSlots);
+        if (!__all_sync(0xffffffffu, split_wait(&sm.iempty[is], (unsigned)(((ni / kTileSlots) & 1) ^ 1), abort, g)))
+          break;
+        ++ni;
+        SplitTileSlot& ts = sm.tile[is];
+        if (lane < 3) reinterpret_cast<int4*>(&ts.rec)[lane] = t4;
+        reinterpret_cast<int4*>(ts.rowoff)[lane] = ro;
+        if (lane < 8) reinterpret_cast<int4*>(ts.coloff)[lane] = co;
+        mbar_arrive(&sm.ifull[is]);  // release: this lane's stores come first
+      }
+      if (pair) {
+        const int es = (int)(q % kExpSlots);
+        if (!__all_sync(0xffffffffu, split_wait(&sm.eempty[es], (unsigned)(((q / kExpSlots) & 1) ^ 1), abort, g)))
+          break;
+        ++q;
+        SplitExpSlot& ex = sm.ex[es];
+        if (lane < 16) reinterpret_cast<int4*>(ex.ea)[lane] = x0;
+        else if (lane < 20) reinterpret_cast<int4*>(ex.eb)[lane - 16] = x0;
+        if (lane < 16) reinterpret_cast<int4*>(ex.sc)[lane] = x1;
+        mbar_arrive(&sm.efull[es]);
+      }
+    }
   } else if (warp < 2 + kEpiWarps) {
     // ---------------------------------------------------------------- epilogue
     const int quarter = warp & 3, cq = (warp - 2) >> 2;
@@ -1022,9 +1114,7 @@ __global__ void __launch_bounds__(kSplitThreads, 1) k_split(const __grid_constan
       int coff[kEpiCols];
 #pragma unroll
       for (int j = 0; j < kEpiCols; ++j) coff[j] = ts.coloff[cq * kEpiCols + j];
-      // the slot is refilled by the async proxy (bulk copy): order this warp's generic reads
-      // of it before the release (write-after-read across proxies needs the proxy fence)
-      fence_proxy_async_smem();
+      // the slot warp refills the slot with ordinary stores after it sees this release
       __syncwarp();
       if (lane == 0) mbar_arrive(&sm.iempty[is]);
       double* cptr = a.C + t.cbase;
@@ -1032,7 +1122,7 @@ __global__ void __launch_bounds__(kSplitThreads, 1) k_split(const __grid_constan
 #pragma unroll
       for (int j = 0; j < kEpiCols; ++j) {
         const bool in = row_in && cq * kEpiCols + j < t.nt;
-        acc[j] = (a.beta_zero || !in) ? 0.0 : __dmul_rn(a.beta, cptr[roff + coff[j]]);
+        acc[j] = (a.beta_zero || !in) ? 0.0 : __dmul_rn(a.beta, __ldcs(cptr + roff + coff[j]));
       }
       const int pe = a.alpha_zero ? t.pb : t.pe;
       for (int p = t.pb; p < pe; ++p, ++q) {
@@ -1051,7 +1141,6 @@ __global__ void __launch_bounds__(kSplitThreads, 1) k_split(const __grid_constan
         const short* fe = &ex.eb[cq * kEpiCols];
         const int er = ex.ea[row];
         auto release_exp = [&]() {
-          fence_proxy_async_smem();  // as for the tile slot
           __syncwarp();
           if (lane == 0) mbar_arrive(&sm.eempty[es]);
         };
@@ -1150,7 +1239,7 @@ __global__ void __launch_bounds__(kSplitThreads, 1) k_split(const __grid_constan
       if (row_in) {
 #pragma unroll
         for (int j = 0; j < kEpiCols; ++j)
-          if (cq * kEpiCols + j < t.nt) cptr[roff + coff[j]] = acc[j];
+          if (cq * kEpiCols + j < t.nt) __stcs(cptr + roff + coff[j], acc[j]);  // streaming: keeps the slices in L2
       }
     }
   }
@@ -1263,7 +1352,22 @@ void split_records(sht_plan* p, cudaStream_t s) {
   const DevSum extra[2] = {{drb.as<long long>() + nc - 1, rm.as<long long>() + nc - 1},
                            {dcb.as<long long>() + nc - 1, rn.as<long long>() + nc - 1}};
   long long h[2] = {0, 0};
-  device_work_list(p, kSplitM, kSplitN, false, s, extra, h, nc > 0 ? 2 : 0);
+  // Many C blocks: order them by A row block (L2 reuse of the A slabs); the tiles are many per
+  // CTA, so the static striding stays balanced.  Few C blocks: heaviest first, for balance.
+  PoolBuf okey;
+  int obits = 0;
+  if (nc >= 16LL * p->ctx->num_sms) {
+    unsigned long long span = 1;
+    for (int t = 0; t < p->tmaps.row.n; ++t) span *= (unsigned long long)C->nblk[p->tmaps.row.y[t]];
+    int rbits = 0;
+    while (rbits < 62 && (1ull << rbits) < span) ++rbits;
+    obits = rbits + 1;
+    okey = PoolBuf(pool, nc * 8, s);
+    k_split_order_keys<<<grid_for(nc, 256), 256, 0, s>>>(C->d_ids.as<long long>(), nc, make_meta(C), p->tmaps.row,
+                                                         p->d_pstart.as<int>(), rbits, okey.as<unsigned long long>());
+    SHT_CUDA(cudaGetLastError());
+  }
+  device_work_list(p, kSplitM, kSplitN, false, s, extra, h, nc > 0 ? 2 : 0, okey.as<unsigned long long>(), obits);
   rtot = h[0];
   ctot = h[1];
   trace("split: work list", s);
