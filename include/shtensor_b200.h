@@ -193,7 +193,10 @@ sht_status sht_set_wait_limit(sht_ctx* ctx, int64_t polls);
 /* ---- diagnostics ---- */
 /* which = 0: FP64 FMA peak of this GPU in TFLOP/s (the FP64 kernels' roofline denominator);
  * which = 1: dense INT8 tensor-core (tcgen05 kind::i8) peak in TOPS (the split kernel's);
- * which = 2: FP64 tensor-core (mma.sync m8n8k4) peak in TFLOP/s (the batched kernel's) */
+ * which = 2: FP64 tensor-core (mma.sync m8n8k4) peak in TFLOP/s (the batched kernel's);
+ * which = 3: the split kernel's operand pipeline alone (stage bulk copies from L2 plus the
+ *            seven-MMA triangle per k-step, 7 slices) in INT8 TOPS: the rate the split kernel
+ *            can reach once its epilogue is hidden */
 sht_status sht_measure_peak(sht_ctx* ctx, int which, double* value);
 
 /* ---- serving loop (no reference counterpart: shtensor has no request loop) ----

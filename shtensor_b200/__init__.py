@@ -467,9 +467,11 @@ def contract(ctx: Context, expr: str, alpha: float, A: Tensor, B: Tensor, beta: 
 
 def measure_peak(ctx: Context, which: str = "fp64") -> float:
     """Roofline denominators measured on this GPU: 'fp64' = FP64 FMA TFLOP/s, 'int8' = dense
-    INT8 tensor-core TOPS, 'dmma' = FP64 tensor-core (m8n8k4) TFLOP/s."""
+    INT8 tensor-core TOPS, 'dmma' = FP64 tensor-core (m8n8k4) TFLOP/s, 'split_pipe' = the split
+    kernel's operand pipeline alone (stage copies from L2 + the 7-slice MMA triangle), INT8 TOPS."""
     v = C.c_double()
-    _check(lib().sht_measure_peak(ctx.handle, {"fp64": 0, "int8": 1, "dmma": 2}[which], C.byref(v)))
+    _check(lib().sht_measure_peak(ctx.handle, {"fp64": 0, "int8": 1, "dmma": 2, "split_pipe": 3}[which],
+                                  C.byref(v)))
     return v.value
 
 

@@ -10,6 +10,7 @@ namespace sht {
 
 double measure_fp64_tflops(sht_ctx* ctx);
 double measure_int8_tops(sht_ctx* ctx);
+double measure_split_pipe_tops(sht_ctx* ctx);
 double measure_dmma_tflops(sht_ctx* ctx);
 void stack_call_static(sht_kernel* k, const double* a, const double* b, double* c, int64_t nb_ops, cudaStream_t s);
 
@@ -659,6 +660,8 @@ sht_status sht_measure_peak(sht_ctx* ctx, int which, double* value) {
       *value = measure_int8_tops(ctx);
     else if (which == 2)
       *value = measure_dmma_tflops(ctx);
+    else if (which == 3)
+      *value = measure_split_pipe_tops(ctx);
     else
       fail(SHT_ERR_UNSUPPORTED, "unknown peak");
   });

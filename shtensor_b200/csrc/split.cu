@@ -350,6 +350,16 @@ __global__ void __launch_bounds__(kSliceWarps * 32, kSliceCtas) k_slice(const __
       row = o.src + o.src_off[cur.b] + (live ? mode_offset(d, st, o.fm, r) : 0);
     }
     auto load_chunk = [&](int c, double (&v)[8]) {
+      if (!hold && k1) {
+        // eight loads from always-valid addresses (k clamped, rows past the block read the
+        // block's start), issued together; the values outside the block are zeroed after
+        double x[8];
+#pragma unroll
+        for (int j = 0; j < 8; ++j) x[j] = row[min(c * 8 + j, K - 1) * kst];
+#pragma unroll
+        for (int j = 0; j < 8; ++j) v[j] = live && c * 8 + j < K ? __dmul_rn(x[j], scale) : 0.0;
+        return;
+      }
 #pragma unroll
       for (int j = 0; j < 8; ++j) {
         const int k = c * 8 + j;
@@ -1655,6 +1665,113 @@ double measure_int8_tops(sht_ctx* ctx) {
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
   if (status) fail(SHT_ERR_TIMEOUT, "INT8 peak probe: a bounded wait on the tensor cores expired");
+  return best;
+}
+
+// ------------------------------------------------------------------ operand pipeline ceiling
+// The split kernel's operand pipeline with nothing after it: per k-step the producer bulk-copies
+// one stage (the A and B slabs of 7 slices, 28 KB + 7 KB, from a buffer resident in L2) into a
+// six-deep ring and the MMA issuer runs the seven-MMA triangle on it (N = 224 .. 32) into one
+// of two TMEM sets.  The stage copies and the tensor core's operand reads share the SM's
+// shared-memory bandwidth, so this rate, not the dense INT8 peak, is what the split kernel can
+// reach per k-step.  Waits are bounded; *status is set if one expires.
+constexpr int kPipeS = 7, kPipeStages = 6, kPipeStage = kPipeS * (kAChunk + kBChunk);
+__global__ void __launch_bounds__(64, 1) k_split_pipe_peak(const signed char* __restrict__ src, long long nstage_src,
+                                                           int iters, long long wait_limit, int* status) {
+  extern __shared__ __align__(1024) unsigned char pipe_smem[];
+  __shared__ __align__(8) unsigned long long full[kPipeStages], empty[kPipeStages], done;
+  __shared__ unsigned tbase;
+  const int tid = threadIdx.x, warp = tid >> 5;
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&tbase)), "r"(512)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  if (tid == 0) {
+    for (int i = 0; i < kPipeStages; ++i) {
+      mbar_init(&full[i], 1);
+      mbar_init(&empty[i], 1);
+    }
+    mbar_init(&done, 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const unsigned tmem = tbase;
+  const unsigned a_bytes = kPipeS * kAChunk, b_bytes = kPipeS * kBChunk;
+  auto wait = [&](unsigned long long* bar, unsigned parity) {
+    for (long long w = 0; w < wait_limit; ++w)
+      if (mbar_try(bar, parity)) return true;
+    atomicExch(status, 1);
+    return false;
+  };
+  if (tid == 0) {
+    int issued = 0;
+    for (int i = 0; i < iters; ++i, ++issued) {
+      const int st = i % kPipeStages;
+      if (i >= kPipeStages && !wait(&empty[st], (unsigned)(((i / kPipeStages) - 1) & 1))) break;
+      const signed char* s = src + ((blockIdx.x * 7919LL + i * 131LL) % nstage_src) * kPipeStage;
+      unsigned char* d = pipe_smem + st * kPipeStage;
+      mbar_expect_tx(&full[st], a_bytes + b_bytes);
+      bulk_g2s(d, s, a_bytes, &full[st]);
+      bulk_g2s(d + a_bytes, s + a_bytes, b_bytes, &full[st]);
+    }
+    // copies still in flight write into shared memory: wait for them before the CTA exits
+    for (int j = issued > kPipeStages ? issued - kPipeStages : 0; j < issued; ++j)
+      wait(&full[j % kPipeStages], (unsigned)((j / kPipeStages) & 1));
+  } else if (tid == 32) {
+    for (int i = 0; i < iters; ++i) {
+      const int st = i % kPipeStages;
+      if (!wait(&full[st], (unsigned)((i / kPipeStages) & 1))) break;
+      tc_fence_after();
+      const unsigned char* a = pipe_smem + st * kPipeStage;
+      const unsigned d = tmem + (unsigned)((i & 1) * (kPipeS * kSplitN + kSplitN));
+#pragma unroll
+      for (int t = 1; t <= kPipeS; ++t)
+        umma_i8(d + (unsigned)((t - 1) * kSplitN), umma_desc(a + (t - 1) * kAChunk), umma_desc(a + a_bytes),
+                idesc_i8(kSplitN * (kPipeS + 1 - t)), t == 1 ? 0 : 1);
+      umma_commit(&empty[st]);
+    }
+    umma_commit(&done);  // every MMA issued has finished before TMEM is released
+    wait(&done, 0);
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 0)
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(512) : "memory");
+}
+
+double measure_split_pipe_tops(sht_ctx* ctx) {
+  const int iters = 4000;
+  const long long nstage_src = (32LL << 20) / kPipeStage;  // 32 MB of slabs: resident in L2
+  PoolBuf src(ctx->pool.get(), nstage_src * kPipeStage, nullptr), st(ctx->pool.get(), 256, nullptr);
+  // non-zero slices (0x5b = 91 in every byte): the tensor core's rate does not depend on zero operands
+  SHT_CUDA(cudaMemsetAsync(src.ptr, 0x5b, nstage_src * kPipeStage, nullptr));
+  SHT_CUDA(cudaMemsetAsync(st.ptr, 0, 4, nullptr));
+  const int smem = kPipeStages * kPipeStage;
+  SHT_CUDA(cudaFuncSetAttribute(k_split_pipe_peak, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+  cudaEvent_t e0, e1;
+  SHT_CUDA(cudaEventCreate(&e0));
+  SHT_CUDA(cudaEventCreate(&e1));
+  double best = 0.0;
+  for (int rep = 0; rep < 4; ++rep) {
+    SHT_CUDA(cudaEventRecord(e0, nullptr));
+    k_split_pipe_peak<<<ctx->num_sms, 64, smem, nullptr>>>(src.as<signed char>(), nstage_src, iters, 1LL << 24,
+                                                           st.as<int>());
+    SHT_CUDA(cudaEventRecord(e1, nullptr));
+    SHT_CUDA(cudaEventSynchronize(e1));
+    float ms = 0;
+    SHT_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+    // the triangle's slice products: 28 of 128 x 32 x 32 per k-step
+    const double ops = 2.0 * kSplitM * (kSplitN * kPipeS * (kPipeS + 1) / 2) * kSplitK * (double)iters * ctx->num_sms;
+    if (rep > 0) best = std::max(best, ops / (ms * 1e-3) / 1e12);
+  }
+  int status = 0;
+  SHT_CUDA(cudaMemcpy(&status, st.ptr, 4, cudaMemcpyDeviceToHost));
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (status) fail(SHT_ERR_TIMEOUT, "split pipeline probe: a bounded wait expired");
   return best;
 }
 

@@ -297,7 +297,19 @@ __global__ void __launch_bounds__(kNormLanes) k_norm_chunks(const T* __restrict_
     const long long end = min(sz, base + kNormChunk);
     const T* p = data + offsets[lo];
     double r = 0.0;
-    for (long long e = base + j; e < end; e += kNormLanes) {
+    long long e = base + j;
+    // eight loads in flight per thread, folded in the same element order as one at a time
+    for (; e + 7 * kNormLanes < end; e += 8 * kNormLanes) {
+      T x[8];
+#pragma unroll
+      for (int u = 0; u < 8; ++u) x[u] = p[e + u * kNormLanes];
+#pragma unroll
+      for (int u = 0; u < 8; ++u) {
+        const double v = (double)x[u];
+        r = maxabs ? fmax(r, fabs(v)) : __fma_rn(v, v, r);
+      }
+    }
+    for (; e < end; e += kNormLanes) {
       const double v = (double)p[e];
       r = maxabs ? fmax(r, fabs(v)) : __fma_rn(v, v, r);
     }

@@ -83,5 +83,8 @@ def test_measured_peaks_are_plausible(ctx):
     assert 100.0 < int8 < 20000.0, int8
     dmma = sht.measure_peak(ctx, "dmma")
     assert 5.0 < dmma < 200.0, dmma
+    # the split kernel's operand pipeline alone: bounded by the dense INT8 rate
+    pipe = sht.measure_peak(ctx, "split_pipe")
+    assert 100.0 < pipe < 1.2 * int8, (pipe, int8)
     v = __import__("ctypes").c_double()
     assert sht.lib().sht_measure_peak(ctx.handle, 7, __import__("ctypes").byref(v)) == sht.Status.ERR_UNSUPPORTED
