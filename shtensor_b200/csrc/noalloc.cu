@@ -12,9 +12,10 @@
 // Set-up: the first call on a device (with that device current) looks up the array's device
 // address with cudaGetSymbolAddress and caches it.  Under CUDA's lazy module loading that
 // first call is also the one that loads this library's module on the device, which commits
-// the 32 MiB array; make that first call outside any stream capture.  All calls share the one array and it keeps the last call's contents: every call
-// rewrites the part it uses (padding included) before reading it, and calls whose work
-// overlaps on the GPU (other streams, or another thread) race on it.
+// the 32 MiB array; make that first call outside any stream capture.  All calls share the one
+// array and it keeps the last call's contents: every call rewrites the part it uses (padding
+// included) before reading it, and calls whose work overlaps on the GPU (other streams, or
+// another thread) race on it.
 #include <cstring>
 #include <map>
 #include <mutex>
