@@ -1053,52 +1053,74 @@ __global__ void __launch_bounds__(kSplitThreads, 1) k_split(const __grid_constan
     // ---------------------------------------------------------------- slot warp
     // Follows the record stream: per tile record it fills a tile slot (the tile's record and
     // its row / column offsets), per pair an exponent slot (row exponents, column exponents,
-    // column scales), 16 bytes per lane.  The loads are issued before the wait for a free
-    // slot, which hides their latency while the warp runs ahead of the epilogue.  Every lane
-    // arrives on the slot's barrier after its own stores.
+    // column scales), 16 bytes per lane.  Two records are in hand at a time: the loads of the
+    // next record are issued before the current one waits for its slots and is stored, so
+    // their latency overlaps.  Every lane arrives on a slot's barrier after its own stores.
+    struct SlotLoad {
+      int4 t4, ro, co, x0, x1;
+      bool first, pair;
+    };
+    auto issue = [&](const SplitRec& v) {
+      SlotLoad d;
+      d.first = (v.kind & kRecFirst) != 0;
+      d.pair = v.ksteps > 0;
+      d.t4 = d.ro = d.co = d.x0 = d.x1 = make_int4(0, 0, 0, 0);
+      if (d.first) {
+        if (lane < 3) d.t4 = reinterpret_cast<const int4*>(v.rec_src)[lane];    // 48-byte record
+        d.ro = reinterpret_cast<const int4*>(v.rowtab_src)[lane];                // 128 row offsets
+        if (lane < 8) d.co = reinterpret_cast<const int4*>(v.coltab_src)[lane];  // 32 column offsets
+      }
+      if (d.pair) {
+        if (lane < 16) d.x0 = reinterpret_cast<const int4*>(v.ae_src)[lane];           // 128 row exponents
+        else if (lane < 20) d.x0 = reinterpret_cast<const int4*>(v.be_src)[lane - 16];  // 32 column exponents
+        if (lane < 16) d.x1 = reinterpret_cast<const int4*>(v.bsc_src)[lane];          // 32 column scales
+      }
+      return d;
+    };
     long long q = 0, ni = 0;
-    for (long long r = 0;; ++r) {
+    auto commit = [&](const SlotLoad& d) {
+      if (d.first) {
+        const int is = (int)(ni % kTileSlots);
+        if (!__all_sync(0xffffffffu, split_wait(&sm.iempty[is], (unsigned)(((ni / kTileSlots) & 1) ^ 1), abort, g)))
+          return false;
+        ++ni;
+        SplitTileSlot& ts = sm.tile[is];
+        if (lane < 3) reinterpret_cast<int4*>(&ts.rec)[lane] = d.t4;
+        reinterpret_cast<int4*>(ts.rowoff)[lane] = d.ro;
+        if (lane < 8) reinterpret_cast<int4*>(ts.coloff)[lane] = d.co;
+        mbar_arrive(&sm.ifull[is]);  // release: this lane's stores come first
+      }
+      if (d.pair) {
+        const int es = (int)(q % kExpSlots);
+        if (!__all_sync(0xffffffffu, split_wait(&sm.eempty[es], (unsigned)(((q / kExpSlots) & 1) ^ 1), abort, g)))
+          return false;
+        ++q;
+        SplitExpSlot& ex = sm.ex[es];
+        if (lane < 16) reinterpret_cast<int4*>(ex.ea)[lane] = d.x0;
+        else if (lane < 20) reinterpret_cast<int4*>(ex.eb)[lane - 16] = d.x0;
+        if (lane < 16) reinterpret_cast<int4*>(ex.sc)[lane] = d.x1;
+        mbar_arrive(&sm.efull[es]);
+      }
+      return true;
+    };
+    SlotLoad cur{};
+    bool have = false, ok = true;
+    for (long long r = 0; ok; ++r) {
       const int rs = (int)(r & (kRecSlots - 1));
-      if (!__all_sync(0xffffffffu, split_wait(&sm.rfull[rs], (unsigned)((r / kRecSlots) & 1), abort, g))) break;
+      if (!__all_sync(0xffffffffu, split_wait(&sm.rfull[rs], (unsigned)((r / kRecSlots) & 1), abort, g))) {
+        ok = false;
+        break;
+      }
       const SplitRec v = sm.rec[rs];
       __syncwarp();
       if (lane == 0) mbar_arrive(&sm.rempty[rs]);
       if (v.kind & kRecEnd) break;
-      const bool first = (v.kind & kRecFirst) != 0, pair = v.ksteps > 0;
-      int4 t4 = make_int4(0, 0, 0, 0), ro = t4, co = t4, x0 = t4, x1 = t4;
-      if (first) {
-        if (lane < 3) t4 = reinterpret_cast<const int4*>(v.rec_src)[lane];       // 48-byte record
-        ro = reinterpret_cast<const int4*>(v.rowtab_src)[lane];                   // 128 row offsets
-        if (lane < 8) co = reinterpret_cast<const int4*>(v.coltab_src)[lane];     // 32 column offsets
-      }
-      if (pair) {
-        if (lane < 16) x0 = reinterpret_cast<const int4*>(v.ae_src)[lane];        // 128 row exponents
-        else if (lane < 20) x0 = reinterpret_cast<const int4*>(v.be_src)[lane - 16];  // 32 column exponents
-        if (lane < 16) x1 = reinterpret_cast<const int4*>(v.bsc_src)[lane];       // 32 column scales
-      }
-      if (first) {
-        const int is = (int)(ni % kTileSlots);
-        if (!__all_sync(0xffffffffu, split_wait(&sm.iempty[is], (unsigned)(((ni / kTileSlots) & 1) ^ 1), abort, g)))
-          break;
-        ++ni;
-        SplitTileSlot& ts = sm.tile[is];
-        if (lane < 3) reinterpret_cast<int4*>(&ts.rec)[lane] = t4;
-        reinterpret_cast<int4*>(ts.rowoff)[lane] = ro;
-        if (lane < 8) reinterpret_cast<int4*>(ts.coloff)[lane] = co;
-        mbar_arrive(&sm.ifull[is]);  // release: this lane's stores come first
-      }
-      if (pair) {
-        const int es = (int)(q % kExpSlots);
-        if (!__all_sync(0xffffffffu, split_wait(&sm.eempty[es], (unsigned)(((q / kExpSlots) & 1) ^ 1), abort, g)))
-          break;
-        ++q;
-        SplitExpSlot& ex = sm.ex[es];
-        if (lane < 16) reinterpret_cast<int4*>(ex.ea)[lane] = x0;
-        else if (lane < 20) reinterpret_cast<int4*>(ex.eb)[lane - 16] = x0;
-        if (lane < 16) reinterpret_cast<int4*>(ex.sc)[lane] = x1;
-        mbar_arrive(&sm.efull[es]);
-      }
+      const SlotLoad nxt = issue(v);
+      if (have) ok = commit(cur);
+      cur = nxt;
+      have = true;
     }
+    if (ok && have) commit(cur);
   } else if (warp < 2 + kEpiWarps) {
     // ---------------------------------------------------------------- epilogue
     const int quarter = warp & 3, cq = (warp - 2) >> 2;
