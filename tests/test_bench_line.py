@@ -59,3 +59,16 @@ def test_cpu_sample_flop_accounting_matches_the_oracle():
     assert 0 < k < n
     rs = oracle.contract(samp.expr, 1.0, bench.host(samp.A), bench.host(samp.B), 0.0, bench.host(samp.C))
     assert np.isclose(fl[:k].sum(), rs.flops, rtol=1e-12) and rs.flops >= 0.3 * r.flops
+
+
+def test_split_roofline_reports_both_ceilings():
+    # the split form's line carries its rate against the dense INT8 peak and against the split
+    # operand-pipeline ceiling, with the slice products credited as 28 per FP64 flop at 7 slices
+    import bench
+    peaks = {"int8": 4000.0, "dmma": 40.0, "split_pipe": 2000.0}
+    r = bench.roofline_of("split", 1e12, 10.0, peaks, S=7)  # 1 TFLOP in 10 ms
+    assert abs(r["fp64_equivalent"]["achieved"] - 100.0) < 1e-9
+    assert abs(r["achieved"] - 2800.0) < 1e-9 and abs(r["frac"] - 0.7) < 1e-12
+    op = r["operand_pipeline"]
+    assert abs(op["frac"] - 1.4) < 1e-12 and op["peak"] == 2000.0 and op["unit"] == "TOPS"
+    assert bench.roofline_of("split", 1e12, 10.0, {"int8": 4000.0}, S=7)["operand_pipeline"]["frac"] is None
